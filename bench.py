@@ -1,0 +1,497 @@
+#!/usr/bin/env python
+"""Benchmark of the gpuNUFFT operator path on B200.
+
+Workload (default): 3D 128^3 image, osf 2, Kaiser-Bessel width 3, sector
+width 8, 32 coils; kooshball trajectory of 8192 spokes x 256 readout points
+(2,097,152 samples, 2D golden-means directions); complex64 N(0,1) k-space;
+32 Gaussian-profile sensitivity maps with random phase ramps, unit
+root-sum-of-squares.  One step = one forward (image -> 32-coil k-space) plus
+one adjoint (32-coil k-space -> coil-combined image).  Synthetic, seeded
+data of the published configuration's shape.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints ONE JSON line (rank 0).  For N > 1 (torchrun) every rank runs an
+independent replica (the path has no cross-GPU exchange); value = all steps
+/ the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = ("fwd+adj/s 3D 128³×32coil batched vs plain; %HBM peak; "
+          "served p99 @1e-5 err")
+UNIT = "fwd+adj/s"
+
+WORKLOADS = {
+    # name: (img dims, n_coils, spokes, readout, osf, kw, sw)
+    "3d128x32": ((128, 128, 128), 32, 8192, 256, 2.0, 3, 8),
+    # small 3D case of the same kernels, for profiler captures
+    "3d64x8": ((64, 64, 64), 8, 2048, 128, 2.0, 3, 8),
+    # 2D single-coil case (upstream CPU-runnable configuration)
+    "2d128x1": ((128, 128), 1, 64, 256, 2.0, 3, 8),
+}
+
+
+def kooshball(n_spokes, n_read):
+    phi1, phi2 = 0.4656, 0.6823
+    m = np.arange(n_spokes)
+    z = (m * phi1) % 1.0 * 2 - 1
+    az = 2 * math.pi * ((m * phi2) % 1.0)
+    s = np.sqrt(np.maximum(0.0, 1 - z * z))
+    d = np.stack([s * np.cos(az), s * np.sin(az), z], 1)
+    r = (np.arange(n_read) - n_read / 2) / n_read
+    k = d[:, None, :] * r[None, :, None]
+    return np.ascontiguousarray(k.reshape(-1, 3).T).astype(np.float32)
+
+
+def radial2d(n_spokes, n_read):
+    ang = np.arange(n_spokes) * (math.pi / ((1 + math.sqrt(5)) / 2))
+    r = (np.arange(n_read) - n_read / 2) / n_read
+    return np.stack([np.outer(np.cos(ang), r).ravel(),
+                     np.outer(np.sin(ang), r).ravel()]).astype(np.float32)
+
+
+def make_inputs(name, seed=0):
+    dims, C, ns, nr, osf, kw, sw = WORKLOADS[name]
+    rng = np.random.default_rng(seed)
+    traj = kooshball(ns, nr) if len(dims) == 3 else radial2d(ns, nr)
+    M = traj.shape[1]
+    shape = tuple(dims[::-1])
+    grids = np.meshgrid(*[np.linspace(-0.5, 0.5, n, dtype=np.float32)
+                          for n in shape], indexing="ij")
+    maps = np.empty((C,) + shape, np.complex64)
+    rss = np.zeros(shape, np.float32)
+    for c in range(C):
+        v = rng.standard_normal(len(shape))
+        cen = 0.6 * v / np.linalg.norm(v)
+        r2 = sum((g - cc) ** 2 for g, cc in zip(grids, cen))
+        ramp = sum(np.float32(rng.uniform(-2, 2)) * g for g in grids)
+        maps[c] = np.exp(-r2 / 0.3) * np.exp(1j * ramp)
+        rss += np.abs(maps[c]) ** 2
+    maps /= np.sqrt(rss)
+    k = (rng.standard_normal((C, M), dtype=np.float32) +
+         1j * rng.standard_normal((C, M), dtype=np.float32)).astype(
+             np.complex64)
+    x = (rng.standard_normal(shape, dtype=np.float32) +
+         1j * rng.standard_normal(shape, dtype=np.float32)).astype(
+             np.complex64)
+    return dict(traj=traj, maps=maps, k=k, x=x, dims=dims, C=C, M=M, osf=osf,
+                kw=kw, sw=sw)
+
+
+# --------------------------------------------------------------------------
+# clocks during the timed region
+# --------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            f = [v.strip() for v in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------------------
+# CPU reference (upstream gpuNUFFT_cpu, built from the upstream sources)
+# --------------------------------------------------------------------------
+def cpu_reference(inp, threads, coils_per_step=None):
+    """Time the upstream CPU gridding routine (adjoint convolution of one
+    coil; the upstream has no CPU forward, FFT or deapodization) on
+    ``threads`` host threads, one coil per thread.  Returns (seconds for
+    one coil pass per thread-slot, coils done)."""
+    from oracle import nufft_oracle as O
+    from oracle import ref
+    if not ref.available():
+        raise RuntimeError("oracle/_ref not built")
+    dims, osf, kw, sw = inp["dims"], inp["osf"], inp["kw"], inp["sw"]
+    if len(dims) == 2:  # exact 3D embedding of the 2D problem (z = 0)
+        traj = np.concatenate([inp["traj"],
+                               np.zeros((1, inp["M"]), np.float32)])
+        gdims = (dims[0], dims[1], dims[0])
+    else:
+        traj, gdims = inp["traj"], dims
+    g = O.make_geometry(gdims, osf, kw, sw)
+    t = O.build_tables(traj, g)
+    lut = O.kernel_lut(osf, kw)
+    crds = np.ascontiguousarray(t.traj_sorted.T)
+    data = [np.ascontiguousarray(inp["k"][c % inp["C"]][t.data_indices])
+            for c in range(threads)]
+    grids = [np.zeros(g.grid_count, np.complex64) for _ in range(threads)]
+
+    def one(i):
+        grids[i][:] = 0
+        ref.cpu_gridding(data[i], crds, lut, t.sector_data_count, t.centers,
+                         sw, kw, g.grid[0], grids[i])
+
+    def step():
+        ths = [threading.Thread(target=one, args=(i,)) for i in
+               range(threads)]
+        t0 = time.perf_counter()
+        for th in ths:
+            th.start()
+        for th in ths:
+            th.join()
+        return time.perf_counter() - t0
+    return step
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, rank):
+    if rank != 0:
+        return
+    inp = make_inputs(args.workload)
+    C = inp["C"]
+    threads = min(cpu_threads(), C)
+    step = cpu_reference(inp, threads)
+    for _ in range(args.warmup):
+        step()
+    ts = [step() for _ in range(args.steps)]
+    per_pass = statistics.mean(ts)  # `threads` coils gridded per step
+    # one fwd+adj on C coils = 2*C gridding passes (forward counted like the
+    # adjoint; FFT, deapodization and coil combine not counted)
+    value = threads / (per_pass * 2 * C)
+    sample = (f"upstream gpuNUFFT_cpu adjoint gridding of {threads} coil(s) "
+              f"per step ({inp['M']} samples each) on {threads} thread(s); "
+              f"fwd+adj/s = coils per second / (2 x {C} coils); FFT and "
+              f"deapodization not counted")
+    line = {"impl": "reference", "metric": METRIC, "value": value,
+            "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": per_pass * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_label(args.workload)},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads,
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_label(name):
+    dims, C, ns, nr, osf, kw, sw = WORKLOADS[name]
+    d = "x".join(str(v) for v in dims)
+    return (f"{len(dims)}D {d} image, {C} coils, osf {osf}, kw {kw}, sw {sw}, "
+            f"{'kooshball' if len(dims) == 3 else 'golden-angle radial'} "
+            f"{ns}x{nr} ({ns * nr} samples), forward + adjoint with coil "
+            f"maps")
+
+
+# --------------------------------------------------------------------------
+# GPU arm
+# --------------------------------------------------------------------------
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """DRAM bytes per launch of the adjoint spread kernel for this workload
+    from the committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get(name, {}).get("adjoint_spread_dram_bytes")
+    except Exception:
+        return None
+
+
+def run_gpu_arm(args, rank, world, dist):
+    import torch
+    import gpunufft_b200 as G
+
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    inp = make_inputs(args.workload, seed=rank)
+    C, M, dims = inp["C"], inp["M"], inp["dims"]
+    plan = G.Plan(inp["traj"], dims, inp["kw"], inp["sw"], inp["osf"], None,
+                  inp["maps"], G.BALANCED, device=dev)
+    x_d = torch.from_numpy(inp["x"]).to(dev)
+    k_d = torch.from_numpy(inp["k"]).to(dev)
+
+    def step():
+        plan.forward(x_d)
+        plan.adjoint(k_d)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    stream = torch.cuda.current_stream()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev) as clk:
+        barrier()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1)
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+
+    # stage times (CUDA events on the plan's launch stream), timed steps
+    plan.set_timing(True)
+    stages = {"fwd": [], "adj": []}
+    launches = 0
+    for _ in range(args.steps):
+        plan.forward(x_d)
+        stages["fwd"].append(plan.stage_times())
+        plan.adjoint(k_d)
+        stages["adj"].append(plan.stage_times())
+    plan.set_timing(False)
+    for v in stages["fwd"] + stages["adj"]:
+        launches += v["launches"]
+    launches_per_step = launches // args.steps
+
+    def avg(kind, key):
+        return statistics.mean(s[key] for s in stages[kind])
+
+    g = plan.info
+    G_cells = int(np.prod([v for v in g.grid_dims if v]))
+    dim = len(dims)
+    spread_ms = avg("adj", "gridding_ms")
+    interp_ms = avg("fwd", "gridding_ms")
+    # algorithmic bytes per launch (k-space read, coordinates, grid write)
+    spread_bytes = 8 * M * C + 4 * dim * M + 8 * G_cells * C
+    interp_bytes = 8 * G_cells * C + 4 * dim * M + 8 * M * C
+    peak, src = peaks()
+    achieved = spread_bytes / (spread_ms * 1e-3) / 1e9
+    traffic = profile_traffic(args.workload)
+
+    # end-to-end through the public API: pinned host inputs -> device,
+    # fwd + adj, results -> pinned host, every step
+    xh = torch.from_numpy(inp["x"]).pin_memory()
+    kh = torch.from_numpy(inp["k"]).pin_memory()
+    out_k = torch.empty((C, M), dtype=torch.complex64).pin_memory()
+    out_x = torch.empty(inp["x"].shape, dtype=torch.complex64).pin_memory()
+
+    def e2e_step():
+        xd = xh.to(dev, non_blocking=True)
+        kd = kh.to(dev, non_blocking=True)
+        kk = plan.forward(xd)
+        ii = plan.adjoint(kd)
+        out_k.copy_(kk, non_blocking=True)
+        out_x.copy_(ii.reshape(out_x.shape), non_blocking=True)
+
+    for _ in range(2):
+        e2e_step()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * args.steps / (e2e_ms / 1e3)
+    h2d = xh.numel() * 8 + kh.numel() * 8
+    d2h = out_k.numel() * 8 + out_x.numel() * 8
+
+    # plain per-call operator (the upstream's flow: one coil per pass, maps
+    # copied per coil per call, a synchronisation per coil)
+    plain_value = None
+    if args.plain_steps > 0:
+        plan_p = G.Plan(inp["traj"], dims, inp["kw"], inp["sw"], inp["osf"],
+                        None, inp["maps"], G.BALANCED, plain=True, device=dev)
+        plan_p.forward(x_d)
+        plan_p.adjoint(k_d)
+        torch.cuda.synchronize()
+        p0 = time.perf_counter()
+        for _ in range(args.plain_steps):
+            plan_p.forward(x_d)
+            plan_p.adjoint(k_d)
+        torch.cuda.synchronize()
+        plain_value = args.plain_steps / (time.perf_counter() - p0)
+        plan_p.close()
+        if dist is not None:
+            t = torch.tensor([plain_value], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MIN)
+            plain_value = float(t.item()) * world
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            threads = min(cpu_threads(), C)
+            step_cpu = cpu_reference(inp, threads)
+            step_cpu()
+            tcpu = statistics.mean(step_cpu() for _ in range(2))
+            cpu_val = threads / (tcpu * 2 * C)
+            cpu = {"value": cpu_val, "unit": UNIT, "cores": threads,
+                   "kind": "reference",
+                   "sample": (f"upstream gpuNUFFT_cpu adjoint gridding, "
+                              f"{threads} coil(s) x 2 steps on {threads} "
+                              f"thread(s); fwd+adj/s = coils/s / (2 x {C}); "
+                              f"FFT and deapodization not counted")}
+        except Exception as e:  # oracle/_ref absent on this machine
+            cpu = {"value": None, "unit": UNIT, "cores": 0,
+                   "kind": "reference", "sample": f"unavailable: {e}"}
+
+    clocks = clk.summary()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": workload_label(args.workload),
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs and grids larger than L2 (126 MB)"},
+            "roofline": {"kernel": "adjoint spread (k_adjoint_spread)",
+                         "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "peak_source": src, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes": spread_bytes,
+                         "launch_ms": spread_ms},
+            "stages_ms": {
+                "forward": {k: avg("fwd", k) for k in
+                            ("prepare_ms", "gridding_ms", "fft_ms",
+                             "finish_ms")},
+                "adjoint": {k: avg("adj", k) for k in
+                            ("prepare_ms", "gridding_ms", "fft_ms",
+                             "finish_ms")},
+                "forward_interp_gbs": interp_bytes / (interp_ms * 1e-3) / 1e9,
+            },
+            "plain": {"value": plain_value, "unit": UNIT,
+                      "steps": args.plain_steps,
+                      "batched_over_plain": (value / plain_value
+                                             if plain_value else None)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "clocks": clocks,
+            "gpu_launches": launches_per_step * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+    plan.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="3d128x32", choices=list(WORKLOADS))
+    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl",
+                                 timeout=datetime.timedelta(seconds=300))
+        dist = tdist
+    try:
+        run_gpu_arm(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

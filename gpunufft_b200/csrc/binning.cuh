@@ -1,0 +1,51 @@
+// Plan-time integer work on the device: sector assignment, stable sort,
+// scans and the per-sector owner candidate lists.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "devutil.hpp"
+#include "geometry.hpp"
+
+namespace gnufft
+{
+
+// Exclusive prefix sum of n u32 values (in may equal out).
+void scan_exclusive(const uint32_t *in, uint32_t *out, size_t n,
+                    cudaStream_t s);
+
+// Stable LSD radix sort of (key, value) pairs on the low `key_bits` bits of
+// the keys.  Sorted output ends in keys_out / vals_out.
+void sort_pairs(const uint32_t *keys_in, const uint32_t *vals_in,
+                uint32_t *keys_out, uint32_t *vals_out, size_t n, int key_bits,
+                cudaStream_t s);
+
+// Counts of `n` keys in [0, bins) -> offsets[bins + 1] (exclusive scan).
+void histogram_offsets(const uint32_t *keys, size_t n, uint32_t bins,
+                       uint32_t *offsets, cudaStream_t s);
+
+// Sector of every sample, original order (assignSectors,
+// gpuNUFFT_operator_factory.cpp:128-181; precomp_kernels.cu:8-45).
+void assign_sectors(const float *traj, uint32_t M, const Geo &g,
+                    uint32_t *sector, cudaStream_t s);
+
+// traj_sorted[a][t] = traj[a][idx[t]]; dens_sorted[t] = dens[idx[t]]
+// (sortArraysKernel, precomp_kernels.cu:85-113).
+void gather_sorted(const float *traj, const float *dens, const uint32_t *idx,
+                   uint32_t M, int dim, float *traj_sorted, float *dens_sorted,
+                   cudaStream_t s);
+
+// Owner candidate lists for the adjoint: for every sector T, the sorted
+// samples whose kernel footprint touches a grid cell owned by T (the cells
+// T*sw .. T*sw+sw-1 per axis, after wrap-around).  Output: cand (values =
+// sorted sample index, grouped by T, ascending within T) and
+// cand_offsets[S + 1].  Returns the number of (sample, owner) pairs.
+size_t build_owner_candidates(const float *traj_sorted,
+                              const uint32_t *sector_sorted, uint32_t M,
+                              const Geo &g, const float *lut,
+                              DeviceBuffer &cand, DeviceBuffer &cand_offsets,
+                              cudaStream_t s);
+
+}  // namespace gnufft

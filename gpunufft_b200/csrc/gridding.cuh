@@ -1,0 +1,86 @@
+// Per-call device kernels of the operator path.
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "geometry.hpp"
+
+namespace gnufft
+{
+
+// Adjoint work item: one owner sector (target) and a slice of its candidate
+// list.  `split` != 0 when the target's candidates are spread over several
+// items; those accumulate into the (pre-zeroed) grid with atomics.
+struct AdjItem
+{
+  int target;
+  int begin;
+  int end;
+  int split;
+};
+
+// Forward work item: samples [begin, end) of one sector.
+struct FwdItem
+{
+  int sector;
+  int begin;
+  int end;
+  int pad_;
+};
+
+// Coil-group width used by the spread / interpolation kernels for C coils.
+int adjoint_coil_group(int C);
+int forward_coil_group(int C, int dim, int pad);
+
+// Dynamic shared memory of the kernels (bytes).
+size_t adjoint_smem_bytes(const Geo &g, int cg);
+size_t forward_smem_bytes(const Geo &g, int cg);
+
+// ks[t*CP + c] = kspace[c*M + idx[t]] * sqrt(dens[t]) (dens may be NULL);
+// zero for C <= c < CP.  (selectOrderedGPU, precomp_kernels.cu:179-205,
+// and performDensityCompensation, std_gpuNUFFT_kernels.cu:220-242.)
+void launch_gather_kspace(const float2 *kspace, const uint32_t *idx,
+                          const float *dens_sorted, uint32_t M, int C, int CP,
+                          float2 *ks, cudaStream_t s);
+
+// Zero the owned cells of the split targets in grid [C][G].
+void launch_zero_split(const int *targets, int n_targets, const Geo &g, int C,
+                       bool shift, float2 *grid, cudaStream_t s);
+
+// Adjoint spread: every target writes its owned cells of grid [C][G] once.
+// With `shift`, cell g is stored at (g - floor(G/2)) mod G per axis (the
+// upstream's INVERSE fftshift ahead of the inverse FFT).
+void launch_adjoint_spread(const AdjItem *items, int n_items,
+                           const uint32_t *cand, const uint32_t *sector_sorted,
+                           const float *traj_sorted, const float2 *ks, int CP,
+                           const Geo &g, const float *lut, uint32_t M, int C,
+                           bool shift, float2 *grid, cudaStream_t s);
+
+// Adjoint finish: crop of the (shifted) inverse-FFT output, 1/sqrt(Ng),
+// deapodization, conj(sens) multiply and coil sum.  stage: 1 = FFT (crop +
+// scale per coil), 2 = DEAPODIZATION.  With `accumulate` (maps only) the
+// coil sum is added to `out` (the upstream's running sum over coil passes).
+void launch_adjoint_finish(const float2 *grid, const float *deapo,
+                           const float2 *sens, const Geo &g, int C, int stage,
+                           bool accumulate, float2 *out, cudaStream_t s);
+
+// Forward prepare: sens multiply, deapodization, zero pad and INVERSE
+// fftshift into grid [C][G].  With `image_grid` the image is written
+// unpadded and unshifted (DENSITY_ESTIMATION, image-sized grid).
+void launch_forward_prepare(const float2 *image, const float2 *sens,
+                            const float *deapo, const Geo &g, int C,
+                            bool image_grid, float2 *grid, cudaStream_t s);
+
+// Forward interpolation from grid [C][G] (the raw FFT output; with `shift`
+// the upstream's FORWARD fftshift is folded into the tile gather), scaled by
+// `scale` and sqrt(dens), scattered to out [C][M] in original order.
+void launch_forward_interp(const FwdItem *items, int n_items,
+                           const float *traj_sorted, const uint32_t *idx,
+                           const float *dens_sorted, const float2 *grid,
+                           const Geo &g, const float *lut, uint32_t M, int C,
+                           bool shift, float scale, float2 *out,
+                           cudaStream_t s);
+
+}  // namespace gnufft

@@ -1,0 +1,989 @@
+// Plan (one per trajectory) and the C ABI declared in include/gpunufft_b200.h.
+//
+// Plan creation restates the upstream factory
+// (gpuNUFFT_operator_factory.cpp:450-553): sector assignment, sort by
+// sector, sorted coordinates / density, sector offsets, centers, balanced
+// processing order and the deapodization function -- and adds the owner
+// candidate lists and work items used by this library's kernels.  All tables
+// stay resident on the device, together with the sensitivity maps, the
+// kernel lookup table and cached cuFFT plans.
+//
+// Calls restate GpuNUFFTOperator::performGpuNUFFTAdj / performForwardGpuNUFFT
+// (gpuNUFFT_operator.cpp:370-1294) with all coils of a call in one pass.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cufft.h>
+#include <cuda_runtime.h>
+
+#include "../../include/gpunufft_b200.h"
+#include "binning.cuh"
+#include "devutil.hpp"
+#include "footprint.cuh"
+#include "geometry.hpp"
+#include "gridding.cuh"
+
+using namespace gnufft;
+
+namespace
+{
+thread_local std::string g_last_error;
+
+// Candidates per adjoint work item and samples per forward work item.
+constexpr int kAdjPayload = 2048;
+constexpr int kFwdPayload = 1024;
+
+// Mirrors the upstream IndPair (gpuNUFFT_types.hpp:33-49): compared by the
+// second member only, so libstdc++'s std::sort produces the upstream order.
+struct SectorPair
+{
+  uint32_t first, second;
+  bool operator<(const SectorPair &o) const { return second < o.second; }
+  bool operator>(const SectorPair &o) const { return second > o.second; }
+};
+
+const char *kVersion = "gpunufft_b200 0.1.0 (sm_100a)";
+
+void check_cufft(cufftResult r, const char *what)
+{
+  if (r != CUFFT_SUCCESS)
+    throw Error(r == CUFFT_ALLOC_FAILED ? kOutOfMemory : kCufftError,
+                std::string(what) + ": cuFFT error " + std::to_string((int)r));
+}
+}  // namespace
+
+struct gnufft_plan
+{
+  gnufft_desc desc{};
+  Geo g{};
+  int dim = 2;
+  uint32_t M = 0;
+  cudaStream_t stream = nullptr;
+  bool texture = false;
+  bool plain = false;
+
+  // host copies of the exported tables
+  std::vector<float> lut_h, traj_sorted_h, dens_sorted_h, deapo_h;
+  std::vector<uint32_t> di_h, sdc_h, centers_h, order_h;
+  bool has_dens = false;
+
+  // resident device tables
+  DeviceBuffer lut, traj_sorted, di, sec_sorted, dens_sorted, cand, cand_off;
+  DeviceBuffer adj_items, split_targets, fwd_items, deapo, sens;
+  int n_adj_items = 0, n_split = 0, n_fwd_items = 0;
+  size_t n_cand = 0;
+  uint32_t sens_coils = 0;
+  std::vector<float2> sens_h;
+
+  // per-call scratch (grow-only)
+  DeviceBuffer ks, grid, stage_in, stage_out, one_sens;
+  std::map<int, cufftHandle> fft;
+
+  // timing
+  bool timing = false;
+  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  gnufft_stage_times times{};
+  uint32_t launches = 0;
+
+  ~gnufft_plan()
+  {
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(desc.device);
+    if (stream)
+      cudaStreamSynchronize(stream);
+    for (auto &kv : fft)
+      cufftDestroy(kv.second);
+    for (auto &e : ev)
+      if (e)
+        cudaEventDestroy(e);
+    if (stream)
+      cudaStreamDestroy(stream);
+    if (prev >= 0)
+      cudaSetDevice(prev);
+  }
+
+  size_t device_bytes() const
+  {
+    const DeviceBuffer *bufs[] = {&lut,         &traj_sorted, &di,
+                                  &sec_sorted,  &dens_sorted, &cand,
+                                  &cand_off,    &adj_items,   &split_targets,
+                                  &fwd_items,   &deapo,       &sens,
+                                  &ks,          &grid,        &stage_in,
+                                  &stage_out,   &one_sens};
+    size_t s = 0;
+    for (auto *b : bufs)
+      s += b->bytes();
+    return s;
+  }
+
+  cufftHandle fft_plan(int batch)
+  {
+    auto it = fft.find(batch);
+    if (it != fft.end())
+      return it->second;
+    cufftHandle h;
+    int n[3];
+    if (dim == 3)
+    {
+      n[0] = g.G[2];
+      n[1] = g.G[1];
+      n[2] = g.G[0];
+    }
+    else
+    {
+      n[0] = g.G[1];
+      n[1] = g.G[0];
+    }
+    check_cufft(cufftPlanMany(&h, dim, n, nullptr, 1, (int)g.grid_count,
+                              nullptr, 1, (int)g.grid_count, CUFFT_C2C, batch),
+                "cufftPlanMany");
+    fft[batch] = h;
+    return h;
+  }
+
+  void mark(int i, cudaStream_t s)
+  {
+    if (timing)
+      GN_CUDA(cudaEventRecord(ev[i], s));
+  }
+};
+
+namespace
+{
+int fail(int st, const std::string &msg)
+{
+  g_last_error = msg;
+  return st;
+}
+
+template <class F> gnufft_status guarded(F &&f)
+{
+  try
+  {
+    f();
+    return GNUFFT_SUCCESS;
+  }
+  catch (const Error &e)
+  {
+    g_last_error = e.what();
+    return (gnufft_status)e.status;
+  }
+  catch (const std::bad_alloc &)
+  {
+    g_last_error = "host allocation failed";
+    return GNUFFT_ERROR_OUT_OF_MEMORY;
+  }
+  catch (const std::exception &e)
+  {
+    g_last_error = e.what();
+    return GNUFFT_ERROR_INTERNAL;
+  }
+}
+
+struct DeviceGuard
+{
+  int prev = -1;
+  explicit DeviceGuard(int dev)
+  {
+    cudaGetDevice(&prev);
+    GN_CUDA(cudaSetDevice(dev));
+  }
+  ~DeviceGuard()
+  {
+    if (prev >= 0)
+      cudaSetDevice(prev);
+  }
+};
+
+template <class T> void upload(DeviceBuffer &b, const T *h, size_t n,
+                               cudaStream_t s)
+{
+  b.reset(std::max<size_t>(n, 1) * sizeof(T));
+  if (n)
+    GN_CUDA(cudaMemcpyAsync(b.get(), h, n * sizeof(T), cudaMemcpyHostToDevice,
+                            s));
+}
+
+template <class T> void download(std::vector<T> &h, const DeviceBuffer &b,
+                                 size_t n, cudaStream_t s)
+{
+  h.resize(n);
+  if (n)
+    GN_CUDA(cudaMemcpyAsync(h.data(), b.get(), n * sizeof(T),
+                            cudaMemcpyDeviceToHost, s));
+}
+
+void validate_desc(const gnufft_desc *d)
+{
+  if (!d)
+    throw Error(kInvalidArgument, "descriptor is NULL");
+  if (d->operator_type < 0 || d->operator_type > 3)
+    throw Error(kInvalidArgument, "unknown operator type");
+  if (d->n_samples == 0)
+    throw Error(kInvalidArgument, "trajectory has no samples");
+}
+
+// computeProcessingOrder (gpuNUFFT_operator_factory.cpp:74-126): sectors by
+// count descending (same libstdc++ std::sort on the same input, so the same
+// order), split into MAXIMUM_PAYLOAD chunks.
+void processing_order(const std::vector<uint32_t> &sdc,
+                      std::vector<uint32_t> &order)
+{
+  std::vector<SectorPair> cps;
+  for (size_t i = 0; i + 1 < sdc.size(); i++)
+    cps.push_back(SectorPair{(uint32_t)i, sdc[i + 1] - sdc[i]});
+  std::sort(cps.begin(), cps.end(), std::greater<SectorPair>());
+  order.clear();
+  for (auto &p : cps)
+  {
+    if (p.second == 0)
+      break;
+    order.push_back(p.first);
+    order.push_back(0);
+    int remaining = (int)p.second;
+    uint32_t off = 1;
+    while (remaining - (int)kUpstreamPayload > 0)
+    {
+      remaining -= kUpstreamPayload;
+      order.push_back(p.first);
+      order.push_back((off++) * kUpstreamPayload);
+    }
+  }
+}
+
+// computeSectorCenters / 2D (gpuNUFFT_operator_factory.cpp:207-270)
+void sector_centers(const Geo &g, std::vector<uint32_t> &c)
+{
+  c.clear();
+  const uint32_t half = (uint32_t)(g.sw >> 1);
+  for (int z = 0; z < (g.dim == 3 ? g.S[2] : 1); ++z)
+    for (int y = 0; y < g.S[1]; ++y)
+      for (int x = 0; x < g.S[0]; ++x)
+      {
+        c.push_back((uint32_t)x * g.sw + half);
+        c.push_back((uint32_t)y * g.sw + half);
+        if (g.dim == 3)
+          c.push_back((uint32_t)z * g.sw + half);
+      }
+}
+
+void build_items(gnufft_plan &p, const std::vector<uint32_t> &cand_off)
+{
+  const int S = p.g.n_sectors;
+  std::vector<AdjItem> split, single;
+  std::vector<int> split_t;
+  for (int t = 0; t < S; ++t)
+  {
+    const uint32_t b = cand_off[t], e = cand_off[t + 1];
+    const uint32_t n = e - b;
+    if (n <= (uint32_t)kAdjPayload)
+    {
+      single.push_back(AdjItem{t, (int)b, (int)e, 0});
+      continue;
+    }
+    split_t.push_back(t);
+    for (uint32_t s = b; s < e; s += kAdjPayload)
+      split.push_back(
+          AdjItem{t, (int)s, (int)std::min<uint32_t>(e, s + kAdjPayload), 1});
+  }
+  std::stable_sort(split.begin(), split.end(),
+                   [](const AdjItem &a, const AdjItem &b) {
+                     return (a.end - a.begin) > (b.end - b.begin);
+                   });
+  std::vector<AdjItem> items(split);
+  items.insert(items.end(), single.begin(), single.end());
+  p.n_adj_items = (int)items.size();
+  p.n_split = (int)split_t.size();
+  upload(p.adj_items, items.data(), items.size(), p.stream);
+  upload(p.split_targets, split_t.data(), split_t.size(), p.stream);
+
+  std::vector<FwdItem> fitems;
+  for (int s = 0; s < S; ++s)
+  {
+    const uint32_t b = p.sdc_h[s], e = p.sdc_h[s + 1];
+    for (uint32_t k = b; k < e; k += kFwdPayload)
+      fitems.push_back(
+          FwdItem{s, (int)k, (int)std::min<uint32_t>(e, k + kFwdPayload), 0});
+  }
+  std::stable_sort(fitems.begin(), fitems.end(),
+                   [](const FwdItem &a, const FwdItem &b) {
+                     return (a.end - a.begin) > (b.end - b.begin);
+                   });
+  p.n_fwd_items = (int)fitems.size();
+  upload(p.fwd_items, fitems.data(), fitems.size(), p.stream);
+}
+
+void init_common(gnufft_plan &p, const gnufft_desc *d)
+{
+  validate_desc(d);
+  p.desc = *d;
+  p.texture = d->operator_type == GNUFFT_TEXTURE ||
+              d->operator_type == GNUFFT_BALANCED_TEXTURE;
+  p.plain = (d->flags & GNUFFT_FLAG_PLAIN) != 0;
+  std::string err;
+  if (!make_geo(d->img_dims, d->osf, d->kernel_width, d->sector_width,
+                p.texture, p.g, err))
+    throw Error(kInvalidArgument, err);
+  p.dim = p.g.dim;
+  p.M = d->n_samples;
+  if ((size_t)p.M * (p.dim + 2) >= (1ull << 31))
+    throw Error(kNotSupported, "too many samples");
+  GN_CUDA(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+  p.lut_h.resize(p.g.lut_len);
+  kernel_lut_fill(p.lut_h.data(), p.g.lut_len, (int)d->kernel_width, d->osf);
+  upload(p.lut, p.lut_h.data(), p.lut_h.size(), p.stream);
+  compute_deapo(p.g, p.lut_h.data(), p.deapo_h);
+  sector_centers(p.g, p.centers_h);
+}
+
+void set_sens_host(gnufft_plan &p, const void *sens, uint32_t n_coils)
+{
+  if (!sens || n_coils == 0)
+  {
+    p.sens_coils = 0;
+    p.sens_h.clear();
+    p.sens.release();
+    return;
+  }
+  const size_t n = (size_t)n_coils * p.g.img_count;
+  const float2 *s = static_cast<const float2 *>(sens);
+  p.sens_h.assign(s, s + n);
+  upload(p.sens, p.sens_h.data(), n, p.stream);
+  p.sens_coils = n_coils;
+}
+
+void finish_tables(gnufft_plan &p)
+{
+  // owner candidates and work items
+  build_owner_candidates(p.traj_sorted.as<float>(), p.sec_sorted.as<uint32_t>(),
+                         p.M, p.g, p.lut.as<float>(), p.cand, p.cand_off,
+                         p.stream);
+  std::vector<uint32_t> cand_off_h;
+  download(cand_off_h, p.cand_off, (size_t)p.g.n_sectors + 1, p.stream);
+  GN_CUDA(cudaStreamSynchronize(p.stream));
+  p.n_cand = cand_off_h.back();
+  build_items(p, cand_off_h);
+  processing_order(p.sdc_h, p.order_h);
+  upload(p.deapo, p.deapo_h.data(), p.deapo_h.size(), p.stream);
+  GN_CUDA(cudaStreamSynchronize(p.stream));
+}
+
+void create_plan(gnufft_plan &p, const gnufft_desc *d, const float *traj,
+                 const float *dens, const void *sens)
+{
+  if (!traj)
+    throw Error(kInvalidArgument, "trajectory is NULL");
+  init_common(p, d);
+  const uint32_t M = p.M;
+  const int dim = p.dim;
+  cudaStream_t s = p.stream;
+
+  DeviceBuffer traj_d, dens_d, sec, iota;
+  upload(traj_d, traj, (size_t)dim * M, s);
+  if (dens)
+  {
+    upload(dens_d, dens, M, s);
+    p.has_dens = true;
+  }
+  sec.reset((size_t)M * sizeof(uint32_t));
+  assign_sectors(traj_d.as<float>(), M, p.g, sec.as<uint32_t>(), s);
+
+  p.di.reset((size_t)M * sizeof(uint32_t));
+  p.sec_sorted.reset((size_t)M * sizeof(uint32_t));
+  if (d->flags & GNUFFT_FLAG_REFERENCE_ORDER)
+  {
+    // the upstream's own order: std::sort of (index, sector) pairs
+    // (sortVector, gpuNUFFT_operator_factory.cpp:56-72)
+    std::vector<uint32_t> sec_h;
+    download(sec_h, sec, M, s);
+    GN_CUDA(cudaStreamSynchronize(s));
+    std::vector<SectorPair> v(M);
+    for (uint32_t i = 0; i < M; ++i)
+      v[i] = SectorPair{i, sec_h[i]};
+    std::sort(v.begin(), v.end());
+    std::vector<uint32_t> di_h(M), ss_h(M);
+    for (uint32_t i = 0; i < M; ++i)
+    {
+      di_h[i] = v[i].first;
+      ss_h[i] = v[i].second;
+    }
+    GN_CUDA(cudaMemcpyAsync(p.di.get(), di_h.data(), M * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s));
+    GN_CUDA(cudaMemcpyAsync(p.sec_sorted.get(), ss_h.data(),
+                            M * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    GN_CUDA(cudaStreamSynchronize(s));
+  }
+  else
+  {
+    std::vector<uint32_t> io(M);
+    for (uint32_t i = 0; i < M; ++i)
+      io[i] = i;
+    upload(iota, io.data(), M, s);
+    int bits = 1;
+    while (bits < 32 && ((uint32_t)(p.g.n_sectors - 1) >> bits))
+      ++bits;
+    sort_pairs(sec.as<uint32_t>(), iota.as<uint32_t>(),
+               p.sec_sorted.as<uint32_t>(), p.di.as<uint32_t>(), M, bits, s);
+  }
+  p.traj_sorted.reset((size_t)dim * M * sizeof(float));
+  if (dens)
+    p.dens_sorted.reset((size_t)M * sizeof(float));
+  gather_sorted(traj_d.as<float>(), dens ? dens_d.as<float>() : nullptr,
+                p.di.as<uint32_t>(), M, dim, p.traj_sorted.as<float>(),
+                dens ? p.dens_sorted.as<float>() : nullptr, s);
+  DeviceBuffer sdc((size_t)(p.g.n_sectors + 1) * sizeof(uint32_t));
+  histogram_offsets(p.sec_sorted.as<uint32_t>(), M, (uint32_t)p.g.n_sectors,
+                    sdc.as<uint32_t>(), s);
+  download(p.sdc_h, sdc, (size_t)p.g.n_sectors + 1, s);
+  download(p.di_h, p.di, M, s);
+  download(p.traj_sorted_h, p.traj_sorted, (size_t)dim * M, s);
+  if (dens)
+    download(p.dens_sorted_h, p.dens_sorted, M, s);
+  GN_CUDA(cudaStreamSynchronize(s));
+  set_sens_host(p, sens, sens ? d->n_coils : 0);
+  finish_tables(p);
+}
+
+void load_plan(gnufft_plan &p, const gnufft_desc *d, const float *traj_sorted,
+               const uint32_t *di, const uint32_t *sdc,
+               const uint32_t *order, uint32_t n_order,
+               const uint32_t *centers, const float *dens_sorted,
+               const void *sens, const float *deapo)
+{
+  if (!traj_sorted || !di || !sdc || !centers || !deapo)
+    throw Error(kInvalidArgument, "precomputed table is NULL");
+  init_common(p, d);
+  const uint32_t M = p.M, S = (uint32_t)p.g.n_sectors;
+  const int dim = p.dim;
+  // validate the tables against the geometry
+  if (sdc[0] != 0 || sdc[S] != M)
+    throw Error(kInvalidArgument, "sector data count does not span samples");
+  for (uint32_t i = 0; i < S; ++i)
+    if (sdc[i + 1] < sdc[i])
+      throw Error(kInvalidArgument, "sector data count not monotone");
+  std::vector<uint8_t> seen(M, 0);
+  for (uint32_t i = 0; i < M; ++i)
+  {
+    if (di[i] >= M || seen[di[i]])
+      throw Error(kInvalidArgument, "data indices are not a permutation");
+    seen[di[i]] = 1;
+  }
+  std::vector<uint32_t> my_centers;
+  sector_centers(p.g, my_centers);
+  if (!std::equal(my_centers.begin(), my_centers.end(), centers))
+    throw Error(kInvalidArgument, "sector centers do not match the geometry");
+  p.sdc_h.assign(sdc, sdc + S + 1);
+  p.di_h.assign(di, di + M);
+  p.traj_sorted_h.assign(traj_sorted, traj_sorted + (size_t)dim * M);
+  p.deapo_h.assign(deapo, deapo + p.g.img_count);
+  std::vector<uint32_t> ss(M);
+  for (uint32_t sct = 0; sct < S; ++sct)
+    for (uint32_t t = sdc[sct]; t < sdc[sct + 1]; ++t)
+      ss[t] = sct;
+  cudaStream_t s = p.stream;
+  upload(p.di, di, M, s);
+  upload(p.sec_sorted, ss.data(), M, s);
+  upload(p.traj_sorted, traj_sorted, (size_t)dim * M, s);
+  if (dens_sorted)
+  {
+    p.has_dens = true;
+    p.dens_sorted_h.assign(dens_sorted, dens_sorted + M);
+    upload(p.dens_sorted, dens_sorted, M, s);
+  }
+  set_sens_host(p, sens, sens ? d->n_coils : 0);
+  finish_tables(p);
+  if (order && n_order)
+    p.order_h.assign(order, order + 2 * (size_t)n_order);
+}
+
+// ------------------------------------------------------------------------
+// per-call execution
+// ------------------------------------------------------------------------
+void check_coils(const gnufft_plan &p, uint32_t C)
+{
+  if (C == 0)
+    throw Error(kInvalidArgument, "n_coils must be positive");
+  if (p.sens_coils && C != p.sens_coils)
+    throw Error(kInvalidArgument,
+                "n_coils differs from the sensitivity map channels");
+}
+
+// All coils of the call in one pass.
+void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
+                     int stage, cudaStream_t s, const float2 *sens,
+                     bool accumulate = false)
+{
+  const Geo &g = p.g;
+  const int cg = adjoint_coil_group((int)C);
+  const int CP = ((int)C + cg - 1) / cg * cg;
+  p.ks.ensure((size_t)p.M * CP * sizeof(float2));
+  const bool conv = stage == GNUFFT_CONVOLUTION ||
+                    stage == GNUFFT_DENSITY_ESTIMATION;
+  float2 *grid = img;
+  if (!conv)
+  {
+    p.grid.ensure((size_t)C * g.grid_count * sizeof(float2));
+    grid = p.grid.as<float2>();
+  }
+  p.mark(0, s);
+  launch_gather_kspace(k, p.di.as<uint32_t>(),
+                       p.has_dens ? p.dens_sorted.as<float>() : nullptr, p.M,
+                       (int)C, CP, p.ks.as<float2>(), s);
+  p.launches += 1;
+  p.mark(1, s);
+  if (p.n_split)
+  {
+    launch_zero_split(p.split_targets.as<int>(), p.n_split, g, (int)C, !conv,
+                      grid, s);
+    p.launches += 1;
+  }
+  launch_adjoint_spread(p.adj_items.as<AdjItem>(), p.n_adj_items,
+                        p.cand.as<uint32_t>(), p.sec_sorted.as<uint32_t>(),
+                        p.traj_sorted.as<float>(), p.ks.as<float2>(), CP, g,
+                        p.lut.as<float>(), p.M, (int)C, !conv, grid, s);
+  p.launches += 1;
+  p.mark(2, s);
+  if (conv)
+  {
+    p.mark(3, s);
+    p.mark(4, s);
+    return;
+  }
+  cufftHandle h = p.fft_plan((int)C);
+  check_cufft(cufftSetStream(h, s), "cufftSetStream");
+  check_cufft(cufftExecC2C(h, (cufftComplex *)grid, (cufftComplex *)grid,
+                           CUFFT_INVERSE),
+              "cufftExecC2C inverse");
+  p.mark(3, s);
+  launch_adjoint_finish(grid, p.deapo.as<float>(),
+                        stage == GNUFFT_DEAPODIZATION ? sens : nullptr, g,
+                        (int)C, stage == GNUFFT_FFT ? 1 : 2, accumulate, img,
+                        s);
+  p.launches += 1;
+  p.mark(4, s);
+}
+
+void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
+                     int stage, cudaStream_t s, const float2 *sens)
+{
+  const Geo &g = p.g;
+  if (stage == GNUFFT_DENSITY_ESTIMATION)
+  {
+    for (int a = 0; a < g.dim; ++a)
+      if (g.N[a] != g.G[a])
+        throw Error(kNotSupported,
+                    "DENSITY_ESTIMATION forward needs grid == image (osf 1)");
+  }
+  p.grid.ensure((size_t)C * g.grid_count * sizeof(float2));
+  float2 *grid = p.grid.as<float2>();
+  const bool dens_est = stage == GNUFFT_DENSITY_ESTIMATION;
+  p.mark(0, s);
+  launch_forward_prepare(img, sens, p.deapo.as<float>(), g, (int)C, dens_est,
+                         grid, s);
+  p.launches += 1;
+  p.mark(1, s);
+  if (!dens_est)
+  {
+    cufftHandle h = p.fft_plan((int)C);
+    check_cufft(cufftSetStream(h, s), "cufftSetStream");
+    check_cufft(cufftExecC2C(h, (cufftComplex *)grid, (cufftComplex *)grid,
+                             CUFFT_FORWARD),
+                "cufftExecC2C forward");
+  }
+  p.mark(2, s);
+  launch_forward_interp(
+      p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
+      p.di.as<uint32_t>(),
+      (p.has_dens && !dens_est) ? p.dens_sorted.as<float>() : nullptr, grid, g,
+      p.lut.as<float>(), p.M, (int)C, !dens_est,
+      dens_est ? 1.0f : g.fft_scale, k, s);
+  p.launches += 1;
+  p.mark(3, s);
+  p.mark(4, s);
+}
+
+size_t adjoint_out_count(const gnufft_plan &p, uint32_t C, int stage)
+{
+  if (stage == GNUFFT_CONVOLUTION || stage == GNUFFT_DENSITY_ESTIMATION)
+    return (size_t)C * p.g.grid_count;
+  if (stage == GNUFFT_DEAPODIZATION && p.sens_coils)
+    return (size_t)p.g.img_count;
+  return (size_t)C * p.g.img_count;
+}
+
+void collect_times(gnufft_plan &p, cudaStream_t s)
+{
+  p.times.launches = p.launches;
+  if (!p.timing)
+    return;
+  GN_CUDA(cudaStreamSynchronize(s));
+  float ms[4] = {0, 0, 0, 0};
+  for (int i = 0; i < 4; ++i)
+    GN_CUDA(cudaEventElapsedTime(&ms[i], p.ev[i], p.ev[i + 1]));
+  p.times.prepare_ms = ms[0];
+  p.times.gridding_ms = ms[1];
+  p.times.fft_ms = ms[2];
+  p.times.finish_ms = ms[3];
+}
+
+// One coil per pass, maps copied per coil per call, a synchronisation per
+// coil (the upstream flow, gpuNUFFT_operator.cpp:682-843 / 941-1051).
+void adjoint_plain(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
+                   int stage, cudaStream_t s, bool host_io)
+{
+  const size_t N = p.g.img_count, G = p.g.grid_count;
+  const bool conv = stage == GNUFFT_CONVOLUTION ||
+                    stage == GNUFFT_DENSITY_ESTIMATION;
+  const bool combine = stage == GNUFFT_DEAPODIZATION && p.sens_coils;
+  const size_t per_out = conv ? G : N;
+  p.stage_in.ensure((size_t)p.M * sizeof(float2));
+  p.stage_out.ensure(per_out * sizeof(float2));
+  DeviceBuffer acc;
+  if (combine)
+  {
+    acc.reset(N * sizeof(float2));
+    GN_CUDA(cudaMemsetAsync(acc.get(), 0, N * sizeof(float2), s));
+    p.one_sens.ensure(N * sizeof(float2));
+  }
+  for (uint32_t c = 0; c < C; ++c)
+  {
+    const float2 *kc = k + (size_t)c * p.M;
+    if (host_io)
+    {
+      GN_CUDA(cudaMemcpyAsync(p.stage_in.get(), kc, p.M * sizeof(float2),
+                              cudaMemcpyHostToDevice, s));
+      kc = p.stage_in.as<float2>();
+    }
+    float2 *oc = host_io ? p.stage_out.as<float2>() : img + c * per_out;
+    if (combine)
+    {
+      // maps copied per coil per call, like the upstream
+      GN_CUDA(cudaMemcpyAsync(p.one_sens.get(), p.sens_h.data() + c * N,
+                              N * sizeof(float2), cudaMemcpyHostToDevice, s));
+      // conj(S_c) * image_c added to the running coil sum
+      adjoint_batched(p, kc, acc.as<float2>(), 1, stage, s,
+                      p.one_sens.as<float2>(), true);
+    }
+    else
+    {
+      adjoint_batched(p, kc, oc, 1, stage, s, nullptr);
+      if (host_io)
+        GN_CUDA(cudaMemcpyAsync(img + c * per_out, oc,
+                                per_out * sizeof(float2),
+                                cudaMemcpyDeviceToHost, s));
+    }
+    GN_CUDA(cudaStreamSynchronize(s));
+  }
+  if (combine)
+    GN_CUDA(cudaMemcpyAsync(img, acc.get(), N * sizeof(float2),
+                            host_io ? cudaMemcpyDeviceToHost
+                                    : cudaMemcpyDeviceToDevice,
+                            s));
+  GN_CUDA(cudaStreamSynchronize(s));
+}
+}  // namespace
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+extern "C" {
+
+const char *gnufft_version(void) { return kVersion; }
+
+const char *gnufft_last_error(void) { return g_last_error.c_str(); }
+
+const char *gnufft_status_string(gnufft_status s)
+{
+  switch (s)
+  {
+  case GNUFFT_SUCCESS: return "success";
+  case GNUFFT_ERROR_INVALID_ARGUMENT: return "invalid argument";
+  case GNUFFT_ERROR_OUT_OF_MEMORY: return "out of memory";
+  case GNUFFT_ERROR_CUDA: return "CUDA error";
+  case GNUFFT_ERROR_CUFFT: return "cuFFT error";
+  case GNUFFT_ERROR_NOT_SUPPORTED: return "not supported";
+  case GNUFFT_ERROR_INTERNAL: return "internal error";
+  }
+  return "unknown status";
+}
+
+gnufft_status gnufft_plan_create(const gnufft_desc *desc, const float *traj,
+                                 const float *dens, const void *sens,
+                                 gnufft_plan **plan)
+{
+  if (!plan)
+    return (gnufft_status)fail(kInvalidArgument, "plan pointer is NULL");
+  *plan = nullptr;
+  return guarded([&] {
+    validate_desc(desc);
+    DeviceGuard dg(desc->device);
+    std::unique_ptr<gnufft_plan> p(new gnufft_plan());
+    p->desc.device = desc->device;
+    create_plan(*p, desc, traj, dens, sens);
+    *plan = p.release();
+  });
+}
+
+gnufft_status gnufft_plan_load(const gnufft_desc *desc,
+                               const float *traj_sorted,
+                               const uint32_t *data_indices,
+                               const uint32_t *sector_data_count,
+                               const uint32_t *processing_order,
+                               uint32_t n_order,
+                               const uint32_t *sector_centers,
+                               const float *dens_sorted, const void *sens,
+                               const float *deapo, gnufft_plan **plan)
+{
+  if (!plan)
+    return (gnufft_status)fail(kInvalidArgument, "plan pointer is NULL");
+  *plan = nullptr;
+  return guarded([&] {
+    validate_desc(desc);
+    DeviceGuard dg(desc->device);
+    std::unique_ptr<gnufft_plan> p(new gnufft_plan());
+    p->desc.device = desc->device;
+    load_plan(*p, desc, traj_sorted, data_indices, sector_data_count,
+              processing_order, n_order, sector_centers, dens_sorted, sens,
+              deapo);
+    *plan = p.release();
+  });
+}
+
+gnufft_status gnufft_plan_destroy(gnufft_plan *plan)
+{
+  return guarded([&] { delete plan; });
+}
+
+gnufft_status gnufft_plan_get_info(const gnufft_plan *p,
+                                   gnufft_plan_info *info)
+{
+  if (!p || !info)
+    return (gnufft_status)fail(kInvalidArgument, "NULL argument");
+  return guarded([&] {
+    std::memset(info, 0, sizeof(*info));
+    info->dim = (uint32_t)p->dim;
+    for (int a = 0; a < 3; ++a)
+    {
+      const bool used = a < p->dim;
+      info->img_dims[a] = used ? (uint32_t)p->g.N[a] : 0;
+      info->grid_dims[a] = used ? (uint32_t)p->g.G[a] : 0;
+      info->sector_dims[a] = used ? (uint32_t)p->g.S[a] : 0;
+    }
+    info->n_sectors = (uint32_t)p->g.n_sectors;
+    info->n_samples = p->M;
+    info->n_coils = p->sens_coils;
+    info->kernel_lut_len = (uint32_t)p->g.lut_len;
+    info->n_processing_order = (uint32_t)(p->order_h.size() / 2);
+    info->has_dens = p->has_dens ? 1 : 0;
+    info->device_bytes = p->device_bytes();
+  });
+}
+
+gnufft_status gnufft_export_tables(const gnufft_plan *p, float *traj_sorted,
+                                   uint32_t *data_indices,
+                                   uint32_t *sector_data_count,
+                                   uint32_t *processing_order,
+                                   uint32_t *sector_centers,
+                                   float *dens_sorted, float *deapo,
+                                   float *kernel_lut)
+{
+  if (!p)
+    return (gnufft_status)fail(kInvalidArgument, "plan is NULL");
+  return guarded([&] {
+    auto cp = [](auto *dst, const auto &v) {
+      if (dst && !v.empty())
+        std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(traj_sorted, p->traj_sorted_h);
+    cp(data_indices, p->di_h);
+    cp(sector_data_count, p->sdc_h);
+    cp(processing_order, p->order_h);
+    cp(sector_centers, p->centers_h);
+    if (p->has_dens)
+      cp(dens_sorted, p->dens_sorted_h);
+    cp(deapo, p->deapo_h);
+    cp(kernel_lut, p->lut_h);
+  });
+}
+
+gnufft_status gnufft_set_sens(gnufft_plan *p, const void *sens,
+                              uint32_t n_coils)
+{
+  if (!p)
+    return (gnufft_status)fail(kInvalidArgument, "plan is NULL");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    GN_CUDA(cudaStreamSynchronize(p->stream));
+    set_sens_host(*p, sens, n_coils);
+    GN_CUDA(cudaStreamSynchronize(p->stream));
+  });
+}
+
+gnufft_status gnufft_set_timing(gnufft_plan *p, int enable)
+{
+  if (!p)
+    return (gnufft_status)fail(kInvalidArgument, "plan is NULL");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    if (enable && !p->ev[0])
+      for (auto &e : p->ev)
+        GN_CUDA(cudaEventCreate(&e));
+    p->timing = enable != 0;
+  });
+}
+
+gnufft_status gnufft_get_stage_times(const gnufft_plan *p,
+                                     gnufft_stage_times *t)
+{
+  if (!p || !t)
+    return (gnufft_status)fail(kInvalidArgument, "NULL argument");
+  *t = p->times;
+  return GNUFFT_SUCCESS;
+}
+
+gnufft_status gnufft_adjoint_device(gnufft_plan *p, const void *kspace,
+                                    void *image, uint32_t n_coils,
+                                    int32_t output, void *stream)
+{
+  if (!p || !kspace || !image)
+    return (gnufft_status)fail(kInvalidArgument, "NULL argument");
+  if (output < 0 || output > 3)
+    return (gnufft_status)fail(kInvalidArgument, "unknown output stage");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    check_coils(*p, n_coils);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    p->launches = 0;
+    if (p->plain)
+      adjoint_plain(*p, (const float2 *)kspace, (float2 *)image, n_coils,
+                    output, s, false);
+    else
+      adjoint_batched(*p, (const float2 *)kspace, (float2 *)image, n_coils,
+                      output, s, p->sens.as<float2>());
+    collect_times(*p, s);
+  });
+}
+
+gnufft_status gnufft_forward_device(gnufft_plan *p, const void *image,
+                                    void *kspace, uint32_t n_coils,
+                                    int32_t output, void *stream)
+{
+  if (!p || !kspace || !image)
+    return (gnufft_status)fail(kInvalidArgument, "NULL argument");
+  if (output < 0 || output > 3)
+    return (gnufft_status)fail(kInvalidArgument, "unknown output stage");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    check_coils(*p, n_coils);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    p->launches = 0;
+    if (p->plain)
+    {
+      const size_t N = p->g.img_count;
+      p->one_sens.ensure(N * sizeof(float2));
+      for (uint32_t c = 0; c < n_coils; ++c)
+      {
+        const float2 *ic = (const float2 *)image;
+        const float2 *sc = nullptr;
+        if (p->sens_coils)
+        {
+          GN_CUDA(cudaMemcpyAsync(p->one_sens.get(), p->sens_h.data() + c * N,
+                                  N * sizeof(float2), cudaMemcpyHostToDevice,
+                                  s));
+          sc = p->one_sens.as<float2>();
+        }
+        else
+          ic += c * N;
+        forward_batched(*p, ic, (float2 *)kspace + (size_t)c * p->M, 1,
+                        output, s, sc);
+        GN_CUDA(cudaStreamSynchronize(s));
+      }
+    }
+    else
+      forward_batched(*p, (const float2 *)image, (float2 *)kspace, n_coils,
+                      output, s, p->sens.as<float2>());
+    collect_times(*p, s);
+  });
+}
+
+gnufft_status gnufft_adjoint_host(gnufft_plan *p, const void *kspace,
+                                  void *image, uint32_t n_coils,
+                                  int32_t output)
+{
+  if (!p || !kspace || !image)
+    return (gnufft_status)fail(kInvalidArgument, "NULL argument");
+  if (output < 0 || output > 3)
+    return (gnufft_status)fail(kInvalidArgument, "unknown output stage");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    check_coils(*p, n_coils);
+    cudaStream_t s = p->stream;
+    p->launches = 0;
+    if (p->plain)
+    {
+      adjoint_plain(*p, (const float2 *)kspace, (float2 *)image, n_coils,
+                    output, s, true);
+      collect_times(*p, s);
+      return;
+    }
+    const size_t nin = (size_t)n_coils * p->M;
+    const size_t nout = adjoint_out_count(*p, n_coils, output);
+    p->stage_in.ensure(nin * sizeof(float2));
+    p->stage_out.ensure(nout * sizeof(float2));
+    GN_CUDA(cudaMemcpyAsync(p->stage_in.get(), kspace, nin * sizeof(float2),
+                            cudaMemcpyHostToDevice, s));
+    adjoint_batched(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
+                    n_coils, output, s, p->sens.as<float2>());
+    GN_CUDA(cudaMemcpyAsync(image, p->stage_out.get(), nout * sizeof(float2),
+                            cudaMemcpyDeviceToHost, s));
+    GN_CUDA(cudaStreamSynchronize(s));
+    collect_times(*p, s);
+  });
+}
+
+gnufft_status gnufft_forward_host(gnufft_plan *p, const void *image,
+                                  void *kspace, uint32_t n_coils,
+                                  int32_t output)
+{
+  if (!p || !kspace || !image)
+    return (gnufft_status)fail(kInvalidArgument, "NULL argument");
+  if (output < 0 || output > 3)
+    return (gnufft_status)fail(kInvalidArgument, "unknown output stage");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    check_coils(*p, n_coils);
+    cudaStream_t s = p->stream;
+    p->launches = 0;
+    const size_t nin =
+        (p->sens_coils ? 1 : (size_t)n_coils) * (size_t)p->g.img_count;
+    const size_t nout = (size_t)n_coils * p->M;
+    p->stage_in.ensure(nin * sizeof(float2));
+    p->stage_out.ensure(nout * sizeof(float2));
+    GN_CUDA(cudaMemcpyAsync(p->stage_in.get(), image, nin * sizeof(float2),
+                            cudaMemcpyHostToDevice, s));
+    if (p->plain)
+    {
+      gnufft_status st = gnufft_forward_device(p, p->stage_in.get(),
+                                               p->stage_out.get(), n_coils,
+                                               output, s);
+      if (st != GNUFFT_SUCCESS)
+        throw Error(st, g_last_error);
+    }
+    else
+      forward_batched(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
+                      n_coils, output, s, p->sens.as<float2>());
+    GN_CUDA(cudaMemcpyAsync(kspace, p->stage_out.get(), nout * sizeof(float2),
+                            cudaMemcpyDeviceToHost, s));
+    GN_CUDA(cudaStreamSynchronize(s));
+    collect_times(*p, s);
+  });
+}
+
+}  // extern "C"

@@ -18,6 +18,8 @@ k-space ``(C, M)`` complex64 in original sample order; images and grids
 """
 from __future__ import annotations
 
+import ctypes
+import ctypes.util
 import math
 from dataclasses import dataclass
 from typing import Optional, Sequence, Tuple
@@ -30,6 +32,28 @@ MAXIMUM_ALIASING_ERROR = f32(0.001)  # gpuNUFFT_utils.hpp:47
 MAXIMUM_ALIASING_ERROR_LIN_INT = f32(0.0001)  # gpuNUFFT_utils.hpp:50
 
 CONVOLUTION, FFT, DEAPODIZATION, DENSITY_ESTIMATION = 0, 1, 2, 3
+
+# The upstream LUT is computed on the host with the C library's float
+# functions; call the same expf / sqrtf so the table is bit-identical (expf
+# is not always correctly rounded).  The compiler turns powf(x, 2) into x*x.
+_libm = ctypes.CDLL(ctypes.util.find_library("m") or "libm.so.6")
+for _fn in ("expf", "sqrtf"):
+    getattr(_libm, _fn).restype = ctypes.c_float
+    getattr(_libm, _fn).argtypes = [ctypes.c_float]
+_libm.powf.restype = ctypes.c_float
+_libm.powf.argtypes = [ctypes.c_float, ctypes.c_float]
+
+
+def _expf(x):
+    return f32(_libm.expf(float(x)))
+
+
+def _sqrtf(x):
+    return f32(_libm.sqrtf(float(x)))
+
+
+def _powf(x, y):
+    return f32(_libm.powf(float(x), float(y)))
 
 
 # --------------------------------------------------------------------------
@@ -61,23 +85,21 @@ def i0_f32(x):
     poly = (f32(0.39894228) + y * (f32(0.1328592e-1) + y * (f32(0.225319e-2) + y * (
         f32(-0.157565e-2) + y * (f32(0.916281e-2) + y * (f32(-0.2057706e-1) + y * (
             f32(0.2635537e-1) + y * (f32(-0.1647633e-1) + y * f32(0.392377e-2)))))))))
-    # expf / sqrtf of glibc are correctly rounded: evaluate in double, round
-    e = f32(math.exp(float(ax)))
-    return f32(f32(e / f32(math.sqrt(float(ax)))) * f32(poly))
+    return f32(f32(_expf(ax) / _sqrtf(ax)) * f32(poly))
 
 
 def beta(kw: int, osf: float) -> np.float32:
     """gpuNUFFT_utils.hpp:60-63 (float32)."""
     osf = f32(osf)
     t = f32(f32(kw) / osf * (osf - f32(0.5)))
-    return f32(f32(math.pi) * f32(math.sqrt(float(f32(t * t - f32(0.8))))))
+    return f32(f32(math.pi) * _sqrtf(f32(t * t - f32(0.8))))
 
 
 def kernel_value(r, kw: int, osf: float) -> np.float32:
     """gpuNUFFT_utils.hpp:72-75: I0(beta*sqrt(1-r^2)) / I0(beta)."""
     b = beta(kw, osf)
     r = f32(r)
-    return f32(i0_f32(f32(b * f32(math.sqrt(float(f32(f32(1.0) - r * r)))))) /
+    return f32(i0_f32(f32(b * _sqrtf(f32(f32(1.0) - r * r)))) /
                i0_f32(b))
 
 
@@ -86,7 +108,7 @@ def lut_size(osf: float, kw: int, lin: bool = False) -> int:
     osf = f32(osf)
     if lin:
         kosf = int(math.floor(math.sqrt(
-            0.37 / (float(osf * osf) * float(MAXIMUM_ALIASING_ERROR_LIN_INT)))))
+            0.37 / float(f32(osf * osf) * MAXIMUM_ALIASING_ERROR_LIN_INT))))
     else:
         kosf = int(math.floor(float(f32(0.91) /
                                     f32(osf * MAXIMUM_ALIASING_ERROR))))

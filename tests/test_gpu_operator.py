@@ -1,0 +1,153 @@
+"""GPU parity of the operator path against the oracle (CPU restatement).
+
+Every call goes through the C ABI (``gpunufft_b200.Plan`` -> ctypes ->
+``libgpunufft_b200.so``).  Tolerances: integer tables bit-exact; floating
+point results within 1e-5 relative L2 of the FP64-accumulating oracle
+(the upstream accumulates in FP32 with atomics in an unspecified order).
+"""
+import numpy as np
+import pytest
+
+from oracle import nufft_oracle as O
+from tests.helpers import cplx, gaussian_maps, kooshball_3d, radial_2d, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+
+def _plan(traj, dims, kw=3, sw=8, osf=2.0, dens=None, sens=None,
+          texture=False, **kw_):
+    import gpunufft_b200 as G
+    op_type = G.BALANCED_TEXTURE if texture else G.BALANCED
+    return G.Plan(traj, dims, kw, sw, osf, dens, sens, op_type, **kw_)
+
+
+CASES = [
+    # (dims, osf, kw, sw, trajectory factory)
+    ((64, 64), 2.0, 3, 8, lambda r: radial_2d(48, 128)),
+    ((48, 40), 1.5, 4, 8, lambda r: r.uniform(-0.5, 0.5, (2, 3000))),
+    ((32, 32), 1.25, 5, 5, lambda r: r.uniform(-0.5, 0.5, (2, 2500))),
+    ((16, 16, 16), 2.0, 3, 8, lambda r: kooshball_3d(200, 32)),
+    ((20, 20, 10), 1.5, 3, 5, lambda r: r.uniform(-0.5, 0.5, (3, 4000))),
+    ((12, 12, 12), 2.0, 4, 3, lambda r: r.uniform(-0.5, 0.5, (3, 1500))),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+def test_tables_bit_exact(case):
+    dims, osf, kw, sw, mk = CASES[case]
+    rng = np.random.default_rng(case)
+    traj = np.asarray(mk(rng), np.float32)
+    p = _plan(traj, dims, kw, sw, osf)
+    t = p.tables()
+    g = O.make_geometry(dims, osf, kw, sw)
+    o = O.build_tables(traj, g)
+    assert np.array_equal(t["sector_data_count"], o.sector_data_count)
+    assert np.array_equal(t["sector_centers"], o.centers)
+    # stable order inside sectors -> identical permutation
+    assert np.array_equal(t["data_indices"], o.data_indices)
+    assert np.array_equal(t["traj_sorted"], o.traj_sorted)
+    assert np.array_equal(t["kernel_lut"], O.kernel_lut(osf, kw))
+    order = t["processing_order"]
+    assert sorted(map(tuple, order)) == sorted(map(tuple, o.order))
+    deapo = O.deapodization(g, O.kernel_lut(osf, kw))
+    assert rel_l2(t["deapo"], deapo.ravel()) < 1e-6
+
+
+@pytest.mark.parametrize("case", range(len(CASES)))
+@pytest.mark.parametrize("n_coils", [1, 3])
+def test_adjoint_forward_vs_oracle(case, n_coils):
+    import gpunufft_b200 as G
+    dims, osf, kw, sw, mk = CASES[case]
+    rng = np.random.default_rng(100 + case)
+    traj = np.asarray(mk(rng), np.float32)
+    M = traj.shape[1]
+    dens = rng.uniform(0.1, 1.0, M).astype(np.float32)
+    p = _plan(traj, dims, kw, sw, osf, dens=dens)
+    ref = O.OracleOperator(traj, dims, kw, sw, osf, dens=dens)
+    k = cplx(rng, n_coils, M)
+    for stage in (G.CONVOLUTION, G.FFT, G.DEAPODIZATION):
+        got = p.adjoint(k, stage)
+        exp = ref.adjoint(k, stage)
+        assert rel_l2(got, exp) < TOL, (stage, rel_l2(got, exp))
+    x = cplx(rng, n_coils, *ref.g.img_shape)
+    got = p.forward(x)
+    exp = ref.forward(x)
+    assert rel_l2(got, exp) < TOL, rel_l2(got, exp)
+
+
+@pytest.mark.parametrize("case", [0, 3, 4])
+def test_sensitivity_combine(case):
+    dims, osf, kw, sw, mk = CASES[case]
+    rng = np.random.default_rng(200 + case)
+    traj = np.asarray(mk(rng), np.float32)
+    M = traj.shape[1]
+    g = O.make_geometry(dims, osf, kw, sw)
+    sens = gaussian_maps(4, g.img_shape, rng)
+    p = _plan(traj, dims, kw, sw, osf, sens=sens)
+    ref = O.OracleOperator(traj, dims, kw, sw, osf, sens=sens)
+    k = cplx(rng, 4, M)
+    assert rel_l2(p.adjoint(k), ref.adjoint(k)) < TOL
+    x = cplx(rng, *g.img_shape)
+    assert rel_l2(p.forward(x), ref.forward(x[None])) < TOL
+
+
+@pytest.mark.parametrize("case", [0, 3])
+def test_texture_variants_vs_oracle(case):
+    dims, osf, kw, sw, mk = CASES[case]
+    rng = np.random.default_rng(300 + case)
+    traj = np.asarray(mk(rng), np.float32)
+    M = traj.shape[1]
+    p = _plan(traj, dims, kw, sw, osf, texture=True)
+    ref = O.OracleOperator(traj, dims, kw, sw, osf, texture=True)
+    k = cplx(rng, 2, M)
+    assert rel_l2(p.adjoint(k), ref.adjoint(k)) < TOL
+    x = cplx(rng, 2, *ref.g.img_shape)
+    assert rel_l2(p.forward(x), ref.forward(x)) < TOL
+
+
+def test_adjointness_device_tensors():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(7)
+    traj = kooshball_3d(400, 48)
+    dims = (24, 24, 24)
+    g = O.make_geometry(dims, 2.0, 3, 8)
+    sens = gaussian_maps(5, g.img_shape, rng)
+    p = _plan(traj, dims, sens=sens)
+    x = torch.from_numpy(cplx(rng, *g.img_shape)).cuda()
+    y = torch.from_numpy(cplx(rng, 5, traj.shape[1])).cuda()
+    ax = p.forward(x)
+    aty = p.adjoint(y)
+    lhs = torch.vdot(ax.reshape(-1).to(torch.complex128),
+                     y.reshape(-1).to(torch.complex128)).item()
+    rhs = torch.vdot(x.reshape(-1).to(torch.complex128),
+                     aty.reshape(-1).to(torch.complex128)).item()
+    assert abs(lhs - rhs) / abs(lhs) < 1e-5
+
+
+def test_nufftop_interface_matches_reference_conventions():
+    import gpunufft_b200 as G
+    rng = np.random.default_rng(11)
+    # the upstream python test: 64x128 image, Cartesian-like lines, 2 coils
+    img_size = [64, 128]
+    ns, nl = img_size[0], img_size[1]
+    loc = np.ones([ns * nl, 2])
+    loc[:, 0] = np.tile(np.linspace(-0.5, 0.5, ns), nl)
+    loc[:, 1] = np.repeat(np.linspace(-0.5, 0.5, nl), ns)
+    loc_arg = np.reshape(loc, loc.shape[::-1], order="F")
+    w = np.ones(loc.shape[0])
+    x, y = np.meshgrid(np.linspace(0, 1, img_size[0]),
+                       np.linspace(0, 1, img_size[1]))
+    m1 = ((1 / (x ** 2 + y ** 2 + 1)).T).astype(np.complex64)
+    maps = np.stack([m1, np.flip(np.flip(m1, 1), 0)])
+    op = G.NUFFTOp(loc_arg, img_size, 2, maps, w, 3, 8, 2, True)
+    img = cplx(rng, *img_size)
+    ks = op.op(np.reshape(img.T, img.size))
+    assert ks.shape == (2, ns * nl)
+    yk = rng.random(ks.shape)
+    adj = op.adj_op(yk)
+    assert adj.shape == (1, 128, 64)
+    lhs = np.vdot(img, np.squeeze(adj).T)
+    rhs = np.vdot(ks, yk)
+    np.testing.assert_allclose(lhs, rhs, rtol=1e-5)

@@ -1,0 +1,136 @@
+"""CPU checks of the oracle: pinned against the upstream's own golden values
+(restated from its gtest suites) and, when ``oracle/_ref`` has been built
+from the upstream sources, against the upstream code itself."""
+import numpy as np
+import pytest
+
+from oracle import nufft_oracle as O
+from oracle import ref
+from tests.helpers import kooshball_3d, radial_2d, rel_l2
+
+needs_ref = pytest.mark.skipif(not ref.available(),
+                               reason="oracle/_ref not built")
+
+
+def test_lut_golden_values():
+    # CUDA/test/cpu/gpuNUFFT_kernel_tests.cpp:8-27 (osf 1, kw 3)
+    k = O.kernel_lut(1.0, 3)
+    assert len(k) == 1365
+    assert k[0] == 1.0 and k[-1] == 0.0
+    assert 0.9940 - k[1] < 1e-4
+    assert 0.0621 - k[401] < 1e-4
+    assert 0.0041 - k[665] < 1e-4
+    # sizes used by the upstream (gpuNUFFT_utils.cpp:47-60)
+    assert O.lut_size(2.0, 3) == 682
+    assert O.lut_size(2.0, 3, lin=True) == 45
+
+
+@needs_ref
+@pytest.mark.parametrize("osf,kw,lin", [(2.0, 3, False), (1.0, 3, False),
+                                        (1.25, 5, False), (1.5, 4, False),
+                                        (2.0, 3, True), (1.25, 5, True)])
+def test_lut_bit_exact_vs_upstream(osf, kw, lin):
+    assert np.array_equal(O.kernel_lut(osf, kw, lin), ref.kernel_lut(osf, kw,
+                                                                     lin))
+
+
+def test_factory_golden_tables():
+    # CUDA/test/cpu/gpuNUFFT_operator_factory_tests.cpp:18-81 (3D)
+    coords = np.array([[-0.5, -0.3, -0.1, 0.1, 0.3, 0.5],
+                       [-0.5, -0.5, 0, 0, 0.5, 0.45],
+                       [-0.33, -0.16666, 0, 0, -0.23, 0.45]], np.float32)
+    g = O.make_geometry((16, 16, 16), 1.5, 3, 8)
+    t = O.build_tables(coords, g)
+    exp = [0, 1, 1, 1, 1, 1, 1, 1, 1, 2, 3, 3, 3, 3, 5, 5, 5, 5, 5, 5, 5, 5,
+           5, 5, 5, 5, 5, 6]
+    assert list(t.sector_data_count) == exp
+    assert g.n_sectors == 27
+    assert list(t.centers[:3]) == [4, 4, 4]
+    assert list(t.data_indices) == [0, 4, 1, 2, 3, 5]
+    assert abs(t.traj_sorted[0, 0] + 0.5) < 1e-4
+    # 2D variant (:113-167)
+    g2 = O.make_geometry((16, 16), 1.5, 3, 8)
+    t2 = O.build_tables(coords[:2], g2)
+    assert list(t2.sector_data_count) == [0, 2, 2, 2, 2, 4, 4, 4, 4, 6]
+    assert g2.n_sectors == 9
+
+
+def test_adjoint_convolution_known_answers():
+    # CUDA/test/gpu/gpuNUFFT_conv_tests.cpp:108-183: one sample at k=0,
+    # 10^3 image, osf 1, kw 3, sw 5 -> 1.0 / 0.4502 / 0.2027
+    g = O.make_geometry((10, 10, 10), 1.0, 3, 5)
+    tab = O.build_tables(np.zeros((3, 1), np.float32), g)
+    grid = O.adjoint_convolution(np.array([[1 + 1j]], np.complex64), tab, g,
+                                 O.kernel_lut(1.0, 3))[0].real
+
+    def at(x, y, z):
+        return grid[x + 10 * (y + 10 * z)]
+    assert abs(at(5, 5, 5) - 1.0) < 1e-4
+    for p in [(5, 4, 5), (4, 5, 5), (5, 6, 5)]:
+        assert abs(at(*p) - 0.4502) < 1e-3
+    for p in [(6, 6, 5), (4, 4, 5), (4, 6, 5)]:
+        assert abs(at(*p) - 0.2027) < 1e-3
+    # :185-283 sample at x=0.4 wraps around (sw 9)
+    g = O.make_geometry((10, 10, 10), 1.0, 3, 9)
+    traj = np.array([[0, 0.4], [0, 0], [0, 0]], np.float32)
+    tab = O.build_tables(traj, g)
+    grid = O.adjoint_convolution(np.array([[1 + 1j, 1 + 1j]], np.complex64),
+                                 tab, g, O.kernel_lut(1.0, 3))[0].real
+    for p in [(9, 4, 5), (8, 5, 5), (9, 6, 5)]:
+        assert abs(at(*p) - 0.4502) < 1e-3
+    for p in [(8, 6, 5), (8, 4, 5), (0, 6, 5)]:
+        assert abs(at(*p) - 0.2027) < 1e-3
+
+
+@needs_ref
+@pytest.mark.parametrize("dims,osf,kw,sw", [
+    ((16, 16, 16), 1.5, 3, 8), ((20, 20, 10), 1.5, 3, 5), ((32, 32), 2.0, 3, 8),
+    ((24, 16), 1.25, 5, 8), ((12, 12, 12), 2.0, 4, 3), ((10, 10, 10), 1.0, 3, 9)])
+def test_tables_bit_exact_vs_upstream(dims, osf, kw, sw):
+    rng = np.random.default_rng(0)
+    dim = len(dims)
+    traj = rng.uniform(-0.5, 0.5, (dim, 3000)).astype(np.float32)
+    traj[:, :50] = np.round(traj[:, :50] * 8) / 8  # exact ties
+    traj[:, 50:60] = 0.5
+    traj[:, 60:70] = -0.5
+    g = O.make_geometry(dims, osf, kw, sw)
+    t = O.build_tables(traj, g)
+    r = ref.sector_tables(traj, dims, osf, kw, sw, balance=True)
+    assert np.array_equal(t.assigned, r["assigned"])
+    assert np.array_equal(t.sector_data_count, r["sector_data_count"])
+    assert np.array_equal(t.centers, r["centers"])
+    sdc = r["sector_data_count"]
+    for i in range(len(sdc) - 1):
+        assert set(t.data_indices[sdc[i]:sdc[i + 1]]) == set(
+            r["data_indices"][sdc[i]:sdc[i + 1]])
+    assert sorted(map(tuple, t.order)) == sorted(map(tuple, r["order"]))
+
+
+@needs_ref
+def test_upstream_cpu_gridding_matches_oracle_interior():
+    # gpuNUFFT_cpu drops out-of-grid cells; compare on a trajectory that stays
+    # away from the grid edge, where both must agree.
+    rng = np.random.default_rng(3)
+    traj = (kooshball_3d(64, 16) * 0.8).astype(np.float32)
+    dims = (16, 16, 16)
+    g = O.make_geometry(dims, 1.0, 3, 8)
+    t = O.build_tables(traj, g)
+    lut = O.kernel_lut(1.0, 3)
+    data = (rng.standard_normal(traj.shape[1]) +
+            1j * rng.standard_normal(traj.shape[1])).astype(np.complex64)
+    got = ref.cpu_gridding(data[t.data_indices], t.traj_sorted.T, lut,
+                           t.sector_data_count, t.centers, 8, 3, 16)
+    exp = O.adjoint_convolution(data[t.data_indices][None], t, g, lut)[0]
+    assert rel_l2(got, exp) < 1e-5
+
+
+def test_operator_matches_direct_nudft():
+    # error of the kw=3, osf=2 operator against the FP64 direct NUDFT
+    rng = np.random.default_rng(5)
+    traj = radial_2d(32, 64)
+    k = (rng.standard_normal(traj.shape[1]) +
+         1j * rng.standard_normal(traj.shape[1])).astype(np.complex64)
+    op = O.OracleOperator(traj, (32, 32), 3, 8, 2.0)
+    got = op.adjoint(k[None])[0] * np.sqrt(op.g.grid_count)
+    exact = O.nudft_adjoint(traj, k, (32, 32))[0]
+    assert rel_l2(got, exact) < 0.05
