@@ -40,7 +40,8 @@ UNIT = "fwd+adj/s"
 WORKLOADS = {
     # name: (img dims, n_coils, spokes, readout, osf, kw, sw)
     "3d128x32": ((128, 128, 128), 32, 8192, 256, 2.0, 3, 8),
-    # small 3D case of the same kernels, for profiler captures
+    # smaller 3D cases of the same kernels, for profiler captures
+    "3d96x32": ((96, 96, 96), 32, 4608, 192, 2.0, 3, 8),
     "3d64x8": ((64, 64, 64), 8, 2048, 128, 2.0, 3, 8),
     # 2D single-coil case (upstream CPU-runnable configuration)
     "2d128x1": ((128, 128), 1, 64, 256, 2.0, 3, 8),

@@ -44,6 +44,27 @@ __device__ __forceinline__ int wrap_mod(int v, int G)
   return v >= G ? v - G : (v < 0 ? v + G : v);
 }
 
+// Asynchronous global -> shared copies (no register round trip, many in
+// flight per thread); completed by cp_async_wait_all() + __syncthreads().
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc)
+{
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s),
+               "l"(gsrc)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all()
+{
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
+
 // --------------------------------------------------------------------------
 // k-space gather into sorted order, coil-interleaved
 // --------------------------------------------------------------------------
@@ -95,129 +116,370 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // --------------------------------------------------------------------------
-// adjoint owner spread
+// compact per-axis footprints (phase A: one sample per thread)
 // --------------------------------------------------------------------------
-template <int DIM>
-__device__ __forceinline__ int owned_axis(float c, int ax, int sec_ax,
-                                          int tgt_ax, const Geo &g,
-                                          const float *lut, int *loc,
-                                          float *w)
+// An axis is described by up to KS (index, weight) entries with static
+// register indices.  Tile frame (forward): the entries are the consecutive
+// cells imin.. of the sample's own tile.  Owner frame (adjoint): the cells,
+// after wrap-around, that lie in the target's sw owned cells, as indices
+// relative to the target's first cell (on grids smaller than a tile plus a
+// footprint these need not be consecutive).
+template <int KS>
+__device__ __forceinline__ int compact_axis(float c, int ax, int sec_ax,
+                                            int tgt_ax, const Geo &g,
+                                            const float *lut, bool owner,
+                                            int *li, float *w)
 {
-  int cells[kSlots];
-  float wt[kSlots];
-  const int n = axis_footprint(c, ax, sec_ax, g, lut, cells, wt);
+  const int center = sec_ax * g.sw + (g.sw >> 1);
+  float pos = __fmaf_rn(c, g.Gf[ax], g.halfG[ax]);
+  pos = __fadd_rn(__fsub_rn(pos, (float)center), (float)g.offset);
+  const int pmax = g.pad - 1;
+  int imin = (int)ceilf(__fsub_rn(pos, g.kernel_radius));
+  int imax = (int)floorf(__fadd_rn(pos, g.kernel_radius));
+  if (imin < 0)
+    imin = 0;
+  if (imax < 0)
+    imax = 0;
+  if (imax >= pmax)
+    imax = pmax;
+  if (imin >= pmax)
+    imin = (int)(pmax - 2 * g.kernel_radius);
+  const int G = g.G[ax];
   const int o = tgt_ax * g.sw;
-  int k = 0;
-  for (int i = 0; i < n; ++i)
+  int n = 0;
+#pragma unroll
+  for (int k = 0; k < KS; ++k)
   {
-    const int l = cells[i] - o;
-    if (l >= 0 && l < g.sw)
-    {
-      loc[k] = l;
-      w[k] = wt[i];
-      ++k;
-    }
+    li[k] = 0;
+    w[k] = 0.0f;
   }
-  return k;
+#pragma unroll
+  for (int k = 0; k < KS; ++k)
+  {
+    const int i = imin + k;
+    const int gc = i + center - g.offset;
+    const float kx = __fsub_rn(__fdiv_rn((float)gc, g.Gf[ax]), 0.5f);
+    const float d = __fmul_rn(__fsub_rn(kx, c), g.aniso[ax]);
+    const float d2 = __fmul_rn(d, d);
+    bool valid = i <= imax && i >= 0;
+    float wt;
+    if (g.texture)
+      wt = lerp_table(lut, g.lut_len, __fmul_rn(d2, g.radius_sq_inv));
+    else
+    {
+      valid = valid && d2 < g.radius_sq;
+      int lx = (int)roundf(__fmul_rn(d2, g.dist_mult));
+      lx = lx < 0 ? 0 : (lx > g.lut_len - 1 ? g.lut_len - 1 : lx);
+      wt = valid ? __ldg(lut + lx) : 0.0f;
+    }
+    int cell = i;  // tile frame
+    if (owner)
+    {
+      int gw = wrap_mod(gc, G);
+      if (gw < 0 || gw >= G)
+        gw = ((gc % G) + G) % G;
+      cell = gw - o;
+      valid = valid && cell >= 0 && cell < g.sw;
+    }
+    // append (static indices only: entry j receives candidate k if j == n)
+#pragma unroll
+    for (int j = 0; j < KS; ++j)
+      if (valid && j == n)
+      {
+        li[j] = cell;
+        w[j] = wt;
+      }
+    n += valid ? 1 : 0;
+  }
+  return n;
 }
 
-template <int DIM, int CG>
-__global__ void __launch_bounds__(kThreads)
+// --------------------------------------------------------------------------
+// adjoint owner spread
+// --------------------------------------------------------------------------
+// Planes of the owned cells (z in 3-D, y rows in 2-D) are grouped in
+// buckets p % 32; unit u (a warp slot of CG coil lanes) owns the buckets
+// b % NU == u, so no two units ever touch the same cell and the shared
+// tile is updated with plain loads and stores.  Phase A lists, per bucket,
+// the (candidate, plane entry) pairs of the chunk in candidate order (warp
+// ballots, deterministic), so phase B visits only its own work.
+//
+// Shared memory: [tile: sw^DIM cells x (CG+1) float2]
+//   [t: CH ints][counts: DIM x CH][indices: DIM x KS x CH]
+//   [weights: DIM x KS x CH floats][lists: NB x CH u16][list counts: NB]
+//   [per-warp bucket counts: NB x 16][k-space rows of the chunk: CH x CG]
+constexpr int kMaxBuckets = 32;
+
+template <int DIM, int CG, int KS>
+__global__ void __launch_bounds__(512)
     k_adjoint_spread(const AdjItem *__restrict__ items,
                      const uint32_t *__restrict__ cand,
                      const uint32_t *__restrict__ sector_sorted,
-                     const float *__restrict__ traj, const float2 *__restrict__ ks,
-                     int CP, Geo g, const float *__restrict__ lut, uint32_t M,
-                     int C, int shift, float2 *__restrict__ grid)
+                     const float *__restrict__ traj,
+                     const float2 *__restrict__ ks, int CP, Geo g,
+                     const float *__restrict__ lut, uint32_t M, int C,
+                     int shift, int CH, float2 *__restrict__ grid)
 {
-  extern __shared__ float2 tile[];  // [sw^DIM][CG + 1]
+  extern __shared__ float2 smem[];
   constexpr int SLOTS = 32 / CG;
   constexpr int PITCH = CG + 1;
+  constexpr int PA = DIM - 1;  // plane axis: z in 3-D, y in 2-D
   const AdjItem it = items[blockIdx.x];
   const int group = blockIdx.y;
   const int sw = g.sw;
   const int cells = DIM == 3 ? sw * sw * sw : sw * sw;
-  for (int i = threadIdx.x; i < cells * PITCH; i += kThreads)
+  const int nthreads = blockDim.x;  // CH <= nthreads candidates per chunk
+  const int nwarps = nthreads >> 5;
+  const int NB = sw < kMaxBuckets ? sw : kMaxBuckets;
+  float2 *tile = smem;
+  int *s_t = reinterpret_cast<int *>(smem + (size_t)cells * PITCH);
+  int *s_n = s_t + CH;             // [DIM][CH]
+  int *s_l = s_n + DIM * CH;       // [DIM][KS][CH]
+  float *s_w = reinterpret_cast<float *>(s_l + DIM * KS * CH);
+  unsigned short *s_list =
+      reinterpret_cast<unsigned short *>(s_w + DIM * KS * CH);  // [NB][CH]
+  int *s_cnt = reinterpret_cast<int *>(s_list + NB * CH + (NB * CH & 1));
+  int *s_wc = s_cnt + NB;          // [NB][16]
+  float2 *s_v = reinterpret_cast<float2 *>(
+      reinterpret_cast<uintptr_t>(s_wc + NB * 16 + 3) & ~uintptr_t(15));
+  for (int i = threadIdx.x; i < cells * PITCH; i += nthreads)
     tile[i] = make_float2(0.f, 0.f);
-
   int ta[3];
   split_sector(it.target, g, ta);
-  __syncthreads();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = lane / CG, coil = lane % CG;
-  const int gcoil = group * CG + coil;
+  const int unit = warp * SLOTS + slot;
+  const int NU = nwarps * SLOTS;
+  const unsigned lt = (1u << lane) - 1u;
 
-  for (int j = it.begin + warp * SLOTS + slot; j < it.end;
-       j += kWarps * SLOTS)
+  for (int base = it.begin; base < it.end; base += CH)
   {
-    const uint32_t t = cand[j];
-    int sa[3];
-    split_sector((int)sector_sorted[t], g, sa);
-    int lx[kSlots], ly[kSlots], lz[kSlots];
-    float wx[kSlots], wy[kSlots], wz[kSlots];
-    const int nx = owned_axis<DIM>(traj[t], 0, sa[0], ta[0], g, lut, lx, wx);
-    const int ny =
-        owned_axis<DIM>(traj[(size_t)M + t], 1, sa[1], ta[1], g, lut, ly, wy);
-    int nz = 1;
-    lz[0] = 0;
-    wz[0] = 1.0f;
-    if (DIM == 3)
-      nz = owned_axis<DIM>(traj[2 * (size_t)M + t], 2, sa[2], ta[2], g, lut,
-                           lz, wz);
-    const float2 v = ks[(size_t)t * CP + gcoil];
-    for (int z = 0; z < nz; ++z)
+    __syncthreads();  // previous chunk consumed, tile zeroed
+    // ---- phase A: footprints of the chunk's candidates, one per thread
+    unsigned bucket_mask = 0;
+    int bucket_entry[KS];
     {
-      for (int y = 0; y < ny; ++y)
-      {
-        // upstream weight order: (K[z] * K[y]) * K[x]
-        const float wzy = DIM == 3 ? __fmul_rn(wz[z], wy[y]) : wy[y];
-        const int rowb = ((DIM == 3 ? lz[z] * sw : 0) + ly[y]) * sw;
-        for (int x = 0; x < nx; ++x)
+      const int j = base + threadIdx.x;
+      const bool holder = threadIdx.x < CH;
+      int t = 0;
+      int nn[3] = {0, 0, 0};
+      int l[3][KS];
+      float w[3][KS];
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
         {
-          const float w = __fmul_rn(wzy, wx[x]);
-          float2 *cell = tile + (size_t)(rowb + lx[x]) * PITCH + coil;
-          atomicAdd(&cell->x, __fmul_rn(w, v.x));
-          atomicAdd(&cell->y, __fmul_rn(w, v.y));
+          l[a][k] = 0;
+          w[a][k] = 0.f;
+        }
+      if (holder && j < it.end)
+      {
+        t = (int)cand[j];
+        int sa[3];
+        split_sector((int)sector_sorted[t], g, sa);
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+          nn[a] = compact_axis<KS>(traj[(size_t)a * M + t], a, sa[a], ta[a],
+                                   g, lut, true, l[a], w[a]);
+      }
+      if (holder)
+      {
+        s_t[threadIdx.x] = t;
+#pragma unroll
+        for (int a = 0; a < DIM; ++a)
+        {
+          s_n[a * CH + threadIdx.x] = nn[a];
+#pragma unroll
+          for (int k = 0; k < KS; ++k)
+          {
+            s_l[(a * KS + k) * CH + threadIdx.x] = l[a][k];
+            s_w[(a * KS + k) * CH + threadIdx.x] = w[a][k];
+          }
+        }
+      }
+      // an owned footprint spans < sw consecutive planes, so each bucket
+      // holds at most one of this candidate's planes
+#pragma unroll
+      for (int k = 0; k < KS; ++k)
+        if (k < nn[PA])
+        {
+          const int b = l[PA][k] % kMaxBuckets;
+          bucket_mask |= 1u << b;
+        }
+#pragma unroll
+      for (int k = 0; k < KS; ++k)
+        bucket_entry[k] = l[PA][k] % kMaxBuckets;
+      for (int b = 0; b < NB; ++b)
+      {
+        const unsigned ball = __ballot_sync(0xffffffffu, (bucket_mask >> b) & 1u);
+        if (lane == 0)
+          s_wc[b * 16 + warp] = __popc(ball);
+      }
+      __syncthreads();
+      if (threadIdx.x < NB)
+      {
+        const int b = threadIdx.x;
+        int acc = 0;
+        for (int w2 = 0; w2 < nwarps; ++w2)
+        {
+          const int c2 = s_wc[b * 16 + w2];
+          s_wc[b * 16 + w2] = acc;
+          acc += c2;
+        }
+        s_cnt[b] = acc;
+      }
+      __syncthreads();
+      for (int b = 0; b < NB; ++b)
+      {
+        const unsigned ball = __ballot_sync(0xffffffffu, (bucket_mask >> b) & 1u);
+        if ((bucket_mask >> b) & 1u)
+        {
+          int e = 0;
+#pragma unroll
+          for (int k = 0; k < KS; ++k)
+            if (k < nn[PA] && bucket_entry[k] == b)
+              e = k;
+          const int pos = s_wc[b * 16 + warp] + __popc(ball & lt);
+          s_list[b * CH + pos] = (unsigned short)((threadIdx.x << 3) | e);
+        }
+      }
+      // stage the chunk's k-space rows (this coil group) in shared memory
+      const int nc = min(CH, it.end - base);
+      constexpr int V4 = CG >= 2 ? CG / 2 : 1;  // 16-byte pieces per row
+      __syncthreads();  // s_t of the chunk visible to every thread
+      for (int q = threadIdx.x; q < nc * V4; q += nthreads)
+      {
+        const int r = q / V4, k = q - r * V4;
+        const float2 *src = ks + (size_t)s_t[r] * CP + group * CG;
+        if (CG >= 2)
+          cp_async16(s_v + r * CG + 2 * k, src + 2 * k);
+        else
+          cp_async8(s_v + r * CG, src);
+      }
+      cp_async_wait_all();
+    }
+    __syncthreads();
+    // ---- phase B: unit u works through the lists of its buckets
+    for (int b = unit; b < NB; b += NU)
+    {
+      const int cnt = s_cnt[b];
+      for (int q = 0; q < cnt; ++q)
+      {
+        const int entry = s_list[b * CH + q];
+        const int i = entry >> 3, e = entry & 7;
+        const int p = s_l[(PA * KS + e) * CH + i];
+        const float wp = s_w[(PA * KS + e) * CH + i];
+        const float2 v = s_v[i * CG + coil];
+        const int nx = s_n[i];
+        int lx[KS];
+        float wx[KS];
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
+        {
+          lx[k] = s_l[k * CH + i];
+          wx[k] = s_w[k * CH + i];
+        }
+        const int ny = DIM == 3 ? s_n[CH + i] : 1;
+        for (int yy = 0; yy < ny; ++yy)
+        {
+          // upstream weight order: (K[z] * K[y]) * K[x]
+          const float wzy =
+              DIM == 3 ? __fmul_rn(wp, s_w[(KS + yy) * CH + i]) : wp;
+          const int row = DIM == 3 ? p * sw + s_l[(KS + yy) * CH + i] : p;
+          float2 *trow = tile + (size_t)row * sw * PITCH + coil;
+          float2 acc[KS];
+#pragma unroll
+          for (int xx = 0; xx < KS; ++xx)
+            if (xx < nx)
+              acc[xx] = trow[(size_t)lx[xx] * PITCH];
+#pragma unroll
+          for (int xx = 0; xx < KS; ++xx)
+            if (xx < nx)
+            {
+              const float wt = __fmul_rn(wzy, wx[xx]);
+              acc[xx].x = __fmaf_rn(wt, v.x, acc[xx].x);
+              acc[xx].y = __fmaf_rn(wt, v.y, acc[xx].y);
+            }
+#pragma unroll
+          for (int xx = 0; xx < KS; ++xx)
+            if (xx < nx)
+              trow[(size_t)lx[xx] * PITCH] = acc[xx];
         }
       }
     }
   }
   __syncthreads();
 
-  // store the owned cells (x fastest) of each coil of the group
+  // store the owned cells of each coil of the group: per-CTA offset tables
+  // (shifted, clipped rows and columns), then division-free loops with
+  // lanes along x
   const long long G = g.grid_count;
-  const int ox = ta[0] * sw, oy = ta[1] * sw, oz = DIM == 3 ? ta[2] * sw : 0;
-  for (int i = threadIdx.x; i < cells * CG; i += kThreads)
+  const int nrows = DIM == 3 ? sw * sw : sw;
+  long long *s_rowoff = reinterpret_cast<long long *>(s_v);  // reuse
+  int *s_xoff = reinterpret_cast<int *>(s_rowoff + nrows);
+  for (int r = threadIdx.x; r < nrows; r += nthreads)
   {
-    const int cl = i / cells;
-    const int cell = i - cl * cells;
-    const int c = group * CG + cl;
-    if (c >= C)
-      continue;
-    const int x = cell % sw;
-    const int y = (cell / sw) % sw;
-    const int z = DIM == 3 ? cell / (sw * sw) : 0;
-    int gx = ox + x, gy = oy + y, gz = oz + z;
-    if (gx >= g.G[0] || gy >= g.G[1] || gz >= g.G[2])
-      continue;
-    if (shift)
+    const int y = r % sw, z = DIM == 3 ? r / sw : 0;
+    int gy = ta[1] * sw + y, gz = DIM == 3 ? ta[2] * sw + z : 0;
+    long long off = -1;
+    if (gy < g.G[1] && gz < g.G[2])
     {
-      gx = wrap_mod(gx - g.shift_inv[0], g.G[0]);
-      gy = wrap_mod(gy - g.shift_inv[1], g.G[1]);
-      gz = DIM == 3 ? wrap_mod(gz - g.shift_inv[2], g.G[2]) : 0;
+      if (shift)
+      {
+        gy = wrap_mod(gy - g.shift_inv[1], g.G[1]);
+        gz = DIM == 3 ? wrap_mod(gz - g.shift_inv[2], g.G[2]) : 0;
+      }
+      off = ((long long)gz * g.G[1] + gy) * g.G[0];
     }
-    const long long q =
-        ((long long)gz * g.G[1] + gy) * g.G[0] + gx + (long long)c * G;
-    const float2 v = tile[(size_t)cell * PITCH + cl];
-    if (it.split)
+    s_rowoff[r] = off;
+  }
+  for (int x = threadIdx.x; x < sw; x += nthreads)
+  {
+    const int gx = ta[0] * sw + x;
+    int off = -1;
+    if (gx < g.G[0])
+      off = shift ? wrap_mod(gx - g.shift_inv[0], g.G[0]) : gx;
+    s_xoff[x] = off;
+  }
+  __syncthreads();
+  {
+    const int lanes_per_row = sw < 32 ? sw : 32;
+    const int x0 = threadIdx.x % lanes_per_row;
+    const int rstep = nthreads / lanes_per_row;
+    const int r0 = threadIdx.x / lanes_per_row;
+    if (r0 < rstep)
     {
-      atomicAdd(&grid[q].x, v.x);
-      atomicAdd(&grid[q].y, v.y);
-    }
-    else
-    {
-      grid[q] = v;
+      for (int cl = 0; cl < CG; ++cl)
+      {
+        const int c = group * CG + cl;
+        if (c >= C)
+          break;
+        float2 *gc = grid + (long long)c * G;
+        for (int r = r0; r < nrows; r += rstep)
+        {
+          const long long ro = s_rowoff[r];
+          if (ro < 0)
+            continue;
+          for (int x = x0; x < sw; x += lanes_per_row)
+          {
+            const int xo = s_xoff[x];
+            if (xo < 0)
+              continue;
+            const float2 v = tile[(size_t)(r * sw + x) * PITCH + cl];
+            if (it.split)
+            {
+              atomicAdd(&gc[ro + xo].x, v.x);
+              atomicAdd(&gc[ro + xo].y, v.y);
+            }
+            else
+            {
+              gc[ro + xo] = v;
+            }
+          }
+        }
+      }
     }
   }
 }
@@ -251,7 +513,9 @@ __global__ void k_zero_split(const int *__restrict__ targets, Geo g, int C,
 // --------------------------------------------------------------------------
 // forward interpolation
 // --------------------------------------------------------------------------
-template <int DIM, int CG>
+// Shared memory: [tile: pad^DIM cells x (CG+1) float2][per-sample geometry
+// (DIM ints) and weights (DIM x KS floats)].
+template <int DIM, int CG, int KS>
 __global__ void __launch_bounds__(kThreads)
     k_forward_interp(const FwdItem *__restrict__ items,
                      const float *__restrict__ traj,
@@ -261,13 +525,17 @@ __global__ void __launch_bounds__(kThreads)
                      const float *__restrict__ lut, uint32_t M, int C,
                      int shift, float scale, float2 *__restrict__ out)
 {
-  extern __shared__ float2 tile[];  // [pad^DIM][CG + 1]
+  extern __shared__ float2 smem[];
   constexpr int SLOTS = 32 / CG;
   constexpr int PITCH = CG + 1;
+  constexpr int CH = kThreads;
   const FwdItem it = items[blockIdx.x];
   const int group = blockIdx.y;
   const int pad = g.pad;
   const int tcells = DIM == 3 ? pad * pad * pad : pad * pad;
+  float2 *tile = smem;
+  int *s_b = reinterpret_cast<int *>(smem + (size_t)tcells * PITCH);
+  float *s_w = reinterpret_cast<float *>(s_b + DIM * CH);
   int sa[3];
   split_sector(it.sector, g, sa);
   int base[3];
@@ -275,83 +543,160 @@ __global__ void __launch_bounds__(kThreads)
     base[a] = sa[a] * g.sw + (g.sw >> 1) - g.offset;
   const long long G = g.grid_count;
 
-  // gather the tile (x fastest) for every coil of the group
-  for (int i = threadIdx.x; i < tcells * CG; i += kThreads)
+  // per-axis source offsets of the tile cells (wrap-around and the
+  // FORWARD fftshift folded in: the value of cell gw sits at gw + ceil(G/2))
+  long long *s_qz = reinterpret_cast<long long *>(
+      reinterpret_cast<uintptr_t>(s_w + DIM * KS * CH + 1) & ~uintptr_t(7));
+  int *s_qy = reinterpret_cast<int *>(s_qz + pad);
+  int *s_qx = s_qy + pad;
+  for (int i = threadIdx.x; i < pad; i += kThreads)
   {
-    const int cl = i / tcells;
-    const int cell = i - cl * tcells;
-    const int c = group * CG + cl;
-    float2 v = make_float2(0.f, 0.f);
-    if (c < C)
+    int q[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
     {
-      const int ix = cell % pad, iy = (cell / pad) % pad;
-      const int iz = DIM == 3 ? cell / (pad * pad) : 0;
-      int q[3];
-      const int li[3] = {ix, iy, iz};
-      for (int a = 0; a < DIM; ++a)
-      {
-        int gc = base[a] + li[a];
-        int gw = wrap_mod(gc, g.G[a]);
-        if (gw < 0 || gw >= g.G[a])
-          gw = ((gc % g.G[a]) + g.G[a]) % g.G[a];
-        if (shift)  // FORWARD fftshift: value of cell gw is at gw + ceil(G/2)
-          gw = wrap_mod(gw + g.shift_fwd[a], g.G[a]);
-        q[a] = gw;
-      }
-      if (DIM == 2)
-        q[2] = 0;
-      v = grid[((long long)q[2] * g.G[1] + q[1]) * g.G[0] + q[0] +
-               (long long)c * G];
+      const int gc = base[a] + i;
+      int gw = wrap_mod(gc, g.G[a]);
+      if (gw < 0 || gw >= g.G[a])
+        gw = ((gc % g.G[a]) + g.G[a]) % g.G[a];
+      if (shift)
+        gw = wrap_mod(gw + g.shift_fwd[a], g.G[a]);
+      q[a] = gw;
     }
-    tile[(size_t)cell * PITCH + cl] = v;
+    s_qx[i] = q[0];
+    s_qy[i] = q[1] * g.G[0];
+    s_qz[i] = DIM == 3 ? (long long)q[2] * g.G[1] * g.G[0] : 0;
   }
   __syncthreads();
+  {
+    const int nrows = DIM == 3 ? pad * pad : pad;
+    const int lanes_per_row = pad < 32 ? pad : 32;
+    const int x0 = threadIdx.x % lanes_per_row;
+    const int rstep = kThreads / lanes_per_row;
+    const int r0 = threadIdx.x / lanes_per_row;
+    if (r0 < rstep)
+    {
+      for (int cl = 0; cl < CG; ++cl)
+      {
+        const int c = group * CG + cl;
+        const float2 *gcp = grid + (long long)c * G;
+        int iy = r0, iz = 0;
+        if (DIM == 3)
+        {
+          iy = r0 % pad;
+          iz = r0 / pad;
+        }
+        const int sy = DIM == 3 ? rstep % pad : 0, sz = DIM == 3 ? rstep / pad : 0;
+        for (int r = r0; r < nrows; r += rstep)
+        {
+          const long long ro = s_qz[iz] + s_qy[iy];
+          for (int x = x0; x < pad; x += lanes_per_row)
+          {
+            float2 *dst = tile + (size_t)(r * pad + x) * PITCH + cl;
+            if (c < C)
+              cp_async8(dst, gcp + ro + s_qx[x]);
+            else
+              *dst = make_float2(0.f, 0.f);
+          }
+          if (DIM == 3)
+          {  // advance (iy, iz) by rstep rows without a division
+            iy += sy;
+            iz += sz;
+            if (iy >= pad)
+            {
+              iy -= pad;
+              ++iz;
+            }
+          }
+          else
+            iy += rstep;
+        }
+      }
+    }
+  }
+  cp_async_wait_all();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = lane / CG, coil = lane % CG;
   const int c = group * CG + coil;
-  for (int t = it.begin + warp * SLOTS + slot; t < it.end;
-       t += kWarps * SLOTS)
+  for (int b0 = it.begin; b0 < it.end; b0 += CH)
   {
-    int cx[kSlots], cy[kSlots], cz[kSlots];
-    int ix[kSlots], iy[kSlots], iz[kSlots];
-    float wx[kSlots], wy[kSlots], wz[kSlots];
-    const int nx = axis_footprint(traj[t], 0, sa[0], g, lut, cx, wx, ix);
-    const int ny =
-        axis_footprint(traj[(size_t)M + t], 1, sa[1], g, lut, cy, wy, iy);
-    int nz = 1;
-    iz[0] = 0;
-    wz[0] = 1.0f;
-    if (DIM == 3)
-      nz = axis_footprint(traj[2 * (size_t)M + t], 2, sa[2], g, lut, cz, wz,
-                          iz);
-    float ax = 0.f, ay = 0.f;
-    for (int z = 0; z < nz; ++z)
-      for (int y = 0; y < ny; ++y)
+    __syncthreads();
+    {
+      const int t = b0 + threadIdx.x;
+#pragma unroll
+      for (int a = 0; a < DIM; ++a)
       {
-        const float wzy = DIM == 3 ? __fmul_rn(wz[z], wy[y]) : wy[y];
-        const int rowb = ((DIM == 3 ? iz[z] * pad : 0) + iy[y]) * pad;
-        for (int x = 0; x < nx; ++x)
+        int l[KS];
+        float w[KS];
+        int nn = 0;
+        if (t < it.end)
+          nn = compact_axis<KS>(traj[(size_t)a * M + t], a, sa[a], 0, g, lut,
+                                false, l, w);
+        // tile frame: entries are consecutive cells starting at l[0]
+        s_b[a * CH + threadIdx.x] = (nn ? l[0] : 0) | (nn << 16);
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
+          s_w[(a * KS + k) * CH + threadIdx.x] = nn ? w[k] : 0.f;
+      }
+    }
+    __syncthreads();
+    const int nc = min(CH, it.end - b0);
+    for (int i = warp * SLOTS + slot; i < nc; i += kWarps * SLOTS)
+    {
+      const int bx = s_b[i], by = s_b[CH + i];
+      const int x0 = bx & 0xffff, nx = bx >> 16;
+      const int y0 = by & 0xffff, ny = by >> 16;
+      int z0 = 0, nz = 1;
+      if (DIM == 3)
+      {
+        const int bz = s_b[2 * CH + i];
+        z0 = bz & 0xffff;
+        nz = bz >> 16;
+      }
+      float wx[KS];
+#pragma unroll
+      for (int k = 0; k < KS; ++k)
+        wx[k] = s_w[k * CH + i];
+      float ax = 0.f, ay = 0.f;
+      for (int z = 0; z < nz; ++z)
+      {
+        const float wz = DIM == 3 ? s_w[(2 * KS + z) * CH + i] : 1.0f;
+        for (int y = 0; y < ny; ++y)
         {
-          const float w = __fmul_rn(wzy, wx[x]);
-          const float2 gv = tile[(size_t)(rowb + ix[x]) * PITCH + coil];
-          ax = __fmaf_rn(gv.x, w, ax);
-          ay = __fmaf_rn(gv.y, w, ay);
+          const float wy = s_w[(KS + y) * CH + i];
+          const float wzy = DIM == 3 ? __fmul_rn(wz, wy) : wy;
+          const int rowb = ((DIM == 3 ? (z0 + z) * pad : 0) + y0 + y) * pad;
+          float2 gv[KS];
+#pragma unroll
+          for (int x = 0; x < KS; ++x)
+            if (x < nx)
+              gv[x] = tile[(size_t)(rowb + x0 + x) * PITCH + coil];
+#pragma unroll
+          for (int x = 0; x < KS; ++x)
+            if (x < nx)
+            {
+              const float w = __fmul_rn(wzy, wx[x]);
+              ax = __fmaf_rn(gv[x].x, w, ax);
+              ay = __fmaf_rn(gv[x].y, w, ay);
+            }
         }
       }
-    if (c < C)
-    {
-      // performFFTScaling then performDensityCompensation
-      // (std_gpuNUFFT_kernels.cu:114-140, 220-242)
-      ax = __fmul_rn(ax, scale);
-      ay = __fmul_rn(ay, scale);
-      if (dens)
+      const int t = b0 + i;
+      if (c < C)
       {
-        const float sd = sqrtf(dens[t]);
-        ax = __fmul_rn(ax, sd);
-        ay = __fmul_rn(ay, sd);
+        // performFFTScaling then performDensityCompensation
+        // (std_gpuNUFFT_kernels.cu:114-140, 220-242)
+        ax = __fmul_rn(ax, scale);
+        ay = __fmul_rn(ay, scale);
+        if (dens)
+        {
+          const float sd = sqrtf(dens[t]);
+          ax = __fmul_rn(ax, sd);
+          ay = __fmul_rn(ay, sd);
+        }
+        out[(size_t)c * M + idx[t]] = make_float2(ax, ay);
       }
-      out[(size_t)c * M + idx[t]] = make_float2(ax, ay);
     }
   }
 }
@@ -419,52 +764,79 @@ __global__ void k_adjoint_finish(const float2 *__restrict__ grid,
   }
 }
 
+// One block per grid row (coil, z, y); threads along x.  Rows whose
+// (shifted) position falls outside the zero-padded image are pure zero
+// stores.
 template <bool SENS>
-__global__ void k_forward_prepare(const float2 *__restrict__ image,
-                                  const float2 *__restrict__ sens,
-                                  const float *__restrict__ deapo, Geo g,
-                                  int image_grid, float2 *__restrict__ grid)
+__global__ void __launch_bounds__(kThreads)
+    k_forward_prepare(const float2 *__restrict__ image,
+                      const float2 *__restrict__ sens,
+                      const float *__restrict__ deapo, Geo g, int C,
+                      int image_grid, float2 *__restrict__ grid)
 {
-  const int c = blockIdx.y;
-  const long long N = g.img_count, G = g.grid_count;
-  const long long total = image_grid ? N : G;
-  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-       q < total; q += (long long)gridDim.x * blockDim.x)
+  const int X = image_grid ? g.N[0] : g.G[0];
+  const int Y = image_grid ? g.N[1] : g.G[1];
+  const int Z = image_grid ? g.N[2] : g.G[2];
+  const long long N = g.img_count;
+  const long long plane = (long long)X * Y * Z;
+  const long long rows = (long long)Y * Z * C;
+  for (long long r = blockIdx.x; r < rows; r += gridDim.x)
   {
-    long long p = q;
-    bool inside = true;
+    const int y = (int)(r % Y);
+    const long long rz = r / Y;
+    const int z = (int)(rz % Z);
+    const int c = (int)(rz / Z);
+    float2 *dst = grid + (long long)c * plane + ((long long)z * Y + y) * X;
+    int py = y, pz = z;
     if (!image_grid)
     {
-      const int qx = (int)(q % g.G[0]);
-      const int qy = (int)((q / g.G[0]) % g.G[1]);
-      const int qz = (int)(q / ((long long)g.G[0] * g.G[1]));
       // INVERSE fftshift of the padded grid: shifted[q] = padded[q+floor(G/2)]
-      const int px = (qx + g.shift_inv[0]) % g.G[0] - g.crop[0];
-      const int py = (qy + g.shift_inv[1]) % g.G[1] - g.crop[1];
-      const int pz = (qz + g.shift_inv[2]) % g.G[2] - g.crop[2];
-      inside = px >= 0 && px < g.N[0] && py >= 0 && py < g.N[1] && pz >= 0 &&
-               pz < g.N[2];
-      p = ((long long)pz * g.N[1] + py) * g.N[0] + px;
+      py = wrap_mod(y + g.shift_inv[1], g.G[1]) - g.crop[1];
+      pz = wrap_mod(z + g.shift_inv[2], g.G[2]) - g.crop[2];
     }
-    float2 v = make_float2(0.f, 0.f);
-    if (inside)
+    const bool row_in = py >= 0 && py < g.N[1] && pz >= 0 && pz < g.N[2];
+    if (!row_in)
     {
-      if (SENS)
-      {  // sensMulKernel (std_gpuNUFFT_kernels.cu:142-156)
-        const float2 a = image[p];
-        const float2 s = sens[p + (long long)c * N];
-        v.x = a.x * s.x - a.y * s.y;
-        v.y = a.x * s.y + a.y * s.x;
+      if ((X & 1) == 0 && ((reinterpret_cast<size_t>(dst) & 15) == 0))
+      {
+        float4 *d4 = reinterpret_cast<float4 *>(dst);
+        for (int x = threadIdx.x; x < X / 2; x += blockDim.x)
+          d4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
       }
       else
       {
-        v = image[p + (long long)c * N];
+        for (int x = threadIdx.x; x < X; x += blockDim.x)
+          dst[x] = make_float2(0.f, 0.f);
       }
-      const float d = deapo[p];
-      v.x = __fmul_rn(v.x, d);
-      v.y = __fmul_rn(v.y, d);
+      continue;
     }
-    grid[q + (long long)c * (image_grid ? N : G)] = v;
+    const long long prow = ((long long)pz * g.N[1] + py) * g.N[0];
+    for (int x = threadIdx.x; x < X; x += blockDim.x)
+    {
+      const int px = image_grid ? x
+                                : wrap_mod(x + g.shift_inv[0], g.G[0]) -
+                                      g.crop[0];
+      float2 v = make_float2(0.f, 0.f);
+      if (px >= 0 && px < g.N[0])
+      {
+        const long long p = prow + px;
+        if (SENS)
+        {  // sensMulKernel (std_gpuNUFFT_kernels.cu:142-156)
+          const float2 a = image[p];
+          const float2 s = sens[p + (long long)c * N];
+          v.x = a.x * s.x - a.y * s.y;
+          v.y = a.x * s.y + a.y * s.x;
+        }
+        else
+        {
+          v = image[p + (long long)c * N];
+        }
+        const float d = deapo[p];
+        v.x = __fmul_rn(v.x, d);
+        v.y = __fmul_rn(v.y, d);
+      }
+      dst[x] = v;
+    }
   }
 }
 
@@ -477,29 +849,33 @@ void set_smem(K kernel, size_t bytes)
                                  (int)bytes));
 }
 
-template <int DIM, int CG>
+template <int DIM, int CG, int KS>
 void adj_dispatch(const AdjItem *items, int n_items, const uint32_t *cand,
                   const uint32_t *sector_sorted, const float *traj,
                   const float2 *ks, int CP, const Geo &g, const float *lut,
                   uint32_t M, int C, bool shift, float2 *grid, cudaStream_t s)
 {
-  const size_t smem = adjoint_smem_bytes(g, CG);
-  auto k = k_adjoint_spread<DIM, CG>;
+  const int threads = adjoint_block_threads(g, CG);
+  int ch = threads;
+  while (ch > 32 && adjoint_smem_bytes(g, CG, ch) > 220 * 1024)
+    ch >>= 1;
+  const size_t smem = adjoint_smem_bytes(g, CG, ch);
+  auto k = k_adjoint_spread<DIM, CG, KS>;
   set_smem(k, smem);
   dim3 grd(n_items, (C + CG - 1) / CG);
-  k<<<grd, kThreads, smem, s>>>(items, cand, sector_sorted, traj, ks, CP, g,
-                                lut, M, C, shift ? 1 : 0, grid);
+  k<<<grd, threads, smem, s>>>(items, cand, sector_sorted, traj, ks, CP, g,
+                               lut, M, C, shift ? 1 : 0, ch, grid);
   GN_LAUNCH_CHECK("adjoint spread");
 }
 
-template <int DIM, int CG>
+template <int DIM, int CG, int KS>
 void fwd_dispatch(const FwdItem *items, int n_items, const float *traj,
                   const uint32_t *idx, const float *dens, const float2 *grid,
                   const Geo &g, const float *lut, uint32_t M, int C,
                   bool shift, float scale, float2 *out, cudaStream_t s)
 {
   const size_t smem = forward_smem_bytes(g, CG);
-  auto k = k_forward_interp<DIM, CG>;
+  auto k = k_forward_interp<DIM, CG, KS>;
   set_smem(k, smem);
   dim3 grd(n_items, (C + CG - 1) / CG);
   k<<<grd, kThreads, smem, s>>>(items, traj, idx, dens, grid, g, lut, M, C,
@@ -514,32 +890,56 @@ int pow2_at_least(int c)
     p <<= 1;
   return p;
 }
+
+// footprint slots per axis: kw + 1 cells
+int slots_for(const Geo &g) { return g.kw + 1 <= 4 ? 4 : 8; }
 }  // namespace
 
 int adjoint_coil_group(int C) { return C > 16 ? 32 : pow2_at_least(C); }
 
 int forward_coil_group(int C, int dim, int pad)
 {
-  int cg = C > 16 ? 32 : pow2_at_least(C);
+  int cg = C > 8 ? 8 : pow2_at_least(C);
   // keep the tile + halo within shared memory
   const size_t cells = dim == 3 ? (size_t)pad * pad * pad : (size_t)pad * pad;
-  while (cg > 1 && cells * (cg + 1) * sizeof(float2) > 200 * 1024)
+  while (cg > 1 && cells * (cg + 1) * sizeof(float2) > 160 * 1024)
     cg >>= 1;
+  if (dim == 2)
+    cg = C > 16 ? 32 : pow2_at_least(C);
   return cg;
 }
 
-size_t adjoint_smem_bytes(const Geo &g, int cg)
+// One unit (warp slot) per owned plane of the target: sw planes.
+int adjoint_block_threads(const Geo &g, int cg)
 {
+  const int slots = 32 / cg;
+  int warps = (g.sw + slots - 1) / slots;
+  warps = warps < 1 ? 1 : (warps > 16 ? 16 : warps);
+  return 32 * warps;
+}
+
+size_t adjoint_smem_bytes(const Geo &g, int cg, int threads)
+{
+  // `threads` = candidates per chunk (CH); per-warp counters sized for 16
   const size_t cells = g.dim == 3 ? (size_t)g.sw * g.sw * g.sw
                                   : (size_t)g.sw * g.sw;
-  return cells * (cg + 1) * sizeof(float2);
+  const int ks = g.kw + 1 <= 4 ? 4 : 8;
+  const int nb = g.sw < 32 ? g.sw : 32;
+  return cells * (cg + 1) * sizeof(float2) +
+         (size_t)threads * (1 + g.dim + 2 * g.dim * ks) * 4 +
+         ((size_t)nb * threads + 1) / 2 * 4 + 4 + (size_t)nb * 17 * 4 + 16 +
+         std::max((size_t)threads * cg * sizeof(float2),
+                  (size_t)(g.dim == 3 ? g.sw * g.sw : g.sw) * 8 +
+                      (size_t)g.sw * 4);
 }
 
 size_t forward_smem_bytes(const Geo &g, int cg)
 {
   const size_t cells = g.dim == 3 ? (size_t)g.pad * g.pad * g.pad
                                   : (size_t)g.pad * g.pad;
-  return cells * (cg + 1) * sizeof(float2);
+  const int ks = g.kw + 1 <= 4 ? 4 : 8;
+  return cells * (cg + 1) * sizeof(float2) +
+         (size_t)kThreads * (g.dim + g.dim * ks) * 4 + 8 + (size_t)g.pad * 16;
 }
 
 void launch_gather_kspace(const float2 *kspace, const uint32_t *idx,
@@ -579,8 +979,12 @@ void launch_adjoint_spread(const AdjItem *items, int n_items,
     return;
   const int cg = adjoint_coil_group(C);
 #define GN_ADJ(D, CGV)                                                         \
-  adj_dispatch<D, CGV>(items, n_items, cand, sector_sorted, traj_sorted, ks,  \
-                       CP, g, lut, M, C, shift, grid, s)
+  if (slots_for(g) == 4)                                                       \
+    adj_dispatch<D, CGV, 4>(items, n_items, cand, sector_sorted, traj_sorted, \
+                            ks, CP, g, lut, M, C, shift, grid, s);            \
+  else                                                                         \
+    adj_dispatch<D, CGV, 8>(items, n_items, cand, sector_sorted, traj_sorted, \
+                            ks, CP, g, lut, M, C, shift, grid, s)
 #define GN_ADJ_CG(D)                                                           \
   switch (cg)                                                                  \
   {                                                                            \
@@ -622,14 +1026,15 @@ void launch_forward_prepare(const float2 *image, const float2 *sens,
                             const float *deapo, const Geo &g, int C,
                             bool image_grid, float2 *grid, cudaStream_t s)
 {
-  const size_t total = image_grid ? (size_t)g.img_count : (size_t)g.grid_count;
-  dim3 grd(grid_for(total, kThreads, 148 * 8), C);
+  const size_t rows = (size_t)C * (image_grid ? (size_t)g.N[1] * g.N[2]
+                                              : (size_t)g.G[1] * g.G[2]);
+  const unsigned nb = (unsigned)std::min<size_t>(rows, 148 * 64);
   if (sens)
-    k_forward_prepare<true><<<grd, kThreads, 0, s>>>(image, sens, deapo, g,
-                                                     image_grid, grid);
+    k_forward_prepare<true><<<nb, kThreads, 0, s>>>(image, sens, deapo, g, C,
+                                                    image_grid, grid);
   else
-    k_forward_prepare<false><<<grd, kThreads, 0, s>>>(image, nullptr, deapo,
-                                                      g, image_grid, grid);
+    k_forward_prepare<false><<<nb, kThreads, 0, s>>>(image, nullptr, deapo, g,
+                                                     C, image_grid, grid);
   GN_LAUNCH_CHECK("forward prepare");
 }
 
@@ -644,8 +1049,12 @@ void launch_forward_interp(const FwdItem *items, int n_items,
     return;
   const int cg = forward_coil_group(C, g.dim, g.pad);
 #define GN_FWD(D, CGV)                                                         \
-  fwd_dispatch<D, CGV>(items, n_items, traj_sorted, idx, dens_sorted, grid, g, \
-                       lut, M, C, shift, scale, out, s)
+  if (slots_for(g) == 4)                                                       \
+    fwd_dispatch<D, CGV, 4>(items, n_items, traj_sorted, idx, dens_sorted,    \
+                            grid, g, lut, M, C, shift, scale, out, s);        \
+  else                                                                         \
+    fwd_dispatch<D, CGV, 8>(items, n_items, traj_sorted, idx, dens_sorted,    \
+                            grid, g, lut, M, C, shift, scale, out, s)
 #define GN_FWD_CG(D)                                                           \
   switch (cg)                                                                  \
   {                                                                            \

@@ -34,8 +34,9 @@ struct FwdItem
 int adjoint_coil_group(int C);
 int forward_coil_group(int C, int dim, int pad);
 
-// Dynamic shared memory of the kernels (bytes).
-size_t adjoint_smem_bytes(const Geo &g, int cg);
+// Launch shape / dynamic shared memory of the kernels.
+int adjoint_block_threads(const Geo &g, int cg);
+size_t adjoint_smem_bytes(const Geo &g, int cg, int chunk);
 size_t forward_smem_bytes(const Geo &g, int cg);
 
 // ks[t*CP + c] = kspace[c*M + idx[t]] * sqrt(dens[t]) (dens may be NULL);

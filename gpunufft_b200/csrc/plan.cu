@@ -87,7 +87,7 @@ struct gnufft_plan
 
   // timing
   bool timing = false;
-  cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t ev[8] = {};  // start / end of prepare, gridding, fft, finish
   gnufft_stage_times times{};
   uint32_t launches = 0;
 
@@ -538,6 +538,7 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
                        (int)C, CP, p.ks.as<float2>(), s);
   p.launches += 1;
   p.mark(1, s);
+  p.mark(2, s);
   if (p.n_split)
   {
     launch_zero_split(p.split_targets.as<int>(), p.n_split, g, (int)C, !conv,
@@ -549,11 +550,13 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
                         p.traj_sorted.as<float>(), p.ks.as<float2>(), CP, g,
                         p.lut.as<float>(), p.M, (int)C, !conv, grid, s);
   p.launches += 1;
-  p.mark(2, s);
+  p.mark(3, s);
+  p.mark(4, s);
   if (conv)
   {
-    p.mark(3, s);
-    p.mark(4, s);
+    p.mark(5, s);
+    p.mark(6, s);
+    p.mark(7, s);
     return;
   }
   cufftHandle h = p.fft_plan((int)C);
@@ -561,13 +564,14 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
   check_cufft(cufftExecC2C(h, (cufftComplex *)grid, (cufftComplex *)grid,
                            CUFFT_INVERSE),
               "cufftExecC2C inverse");
-  p.mark(3, s);
+  p.mark(5, s);
+  p.mark(6, s);
   launch_adjoint_finish(grid, p.deapo.as<float>(),
                         stage == GNUFFT_DEAPODIZATION ? sens : nullptr, g,
                         (int)C, stage == GNUFFT_FFT ? 1 : 2, accumulate, img,
                         s);
   p.launches += 1;
-  p.mark(4, s);
+  p.mark(7, s);
 }
 
 void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
@@ -589,6 +593,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
                          grid, s);
   p.launches += 1;
   p.mark(1, s);
+  p.mark(4, s);
   if (!dens_est)
   {
     cufftHandle h = p.fft_plan((int)C);
@@ -597,6 +602,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
                              CUFFT_FORWARD),
                 "cufftExecC2C forward");
   }
+  p.mark(5, s);
   p.mark(2, s);
   launch_forward_interp(
       p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
@@ -606,7 +612,8 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
       dens_est ? 1.0f : g.fft_scale, k, s);
   p.launches += 1;
   p.mark(3, s);
-  p.mark(4, s);
+  p.mark(6, s);
+  p.mark(7, s);
 }
 
 size_t adjoint_out_count(const gnufft_plan &p, uint32_t C, int stage)
@@ -626,7 +633,7 @@ void collect_times(gnufft_plan &p, cudaStream_t s)
   GN_CUDA(cudaStreamSynchronize(s));
   float ms[4] = {0, 0, 0, 0};
   for (int i = 0; i < 4; ++i)
-    GN_CUDA(cudaEventElapsedTime(&ms[i], p.ev[i], p.ev[i + 1]));
+    GN_CUDA(cudaEventElapsedTime(&ms[i], p.ev[2 * i], p.ev[2 * i + 1]));
   p.times.prepare_ms = ms[0];
   p.times.gridding_ms = ms[1];
   p.times.fft_ms = ms[2];
