@@ -261,6 +261,65 @@ __global__ void k_owner_pairs(const float *__restrict__ traj_sorted,
   }
 }
 
+// Every (cell, weight) of the footprint of sorted sample t.
+template <bool FILL>
+__global__ void k_interp_pairs(const float *__restrict__ traj_sorted,
+                               const uint32_t *__restrict__ sector_sorted,
+                               uint32_t M, Geo g, const float *__restrict__ lut,
+                               uint32_t *__restrict__ count,
+                               const uint32_t *__restrict__ pos,
+                               uint32_t *__restrict__ keys,
+                               uint32_t *__restrict__ ids,
+                               uint2 *__restrict__ pairs)
+{
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < M;
+       t += (size_t)gridDim.x * blockDim.x)
+  {
+    int sa[3];
+    split_sector(sector_sorted[t], g, sa);
+    int cell[3][kSlots];
+    float w[3][kSlots];
+    int n[3] = {1, 1, 1};
+    cell[2][0] = 0;
+    w[2][0] = 1.0f;
+    for (int a = 0; a < g.dim; ++a)
+      n[a] = axis_footprint(traj_sorted[(size_t)a * M + t], a, sa[a], g, lut,
+                            cell[a], w[a]);
+    if (!FILL)
+    {
+      count[t] = (uint32_t)(n[0] * n[1] * n[2]);
+      continue;
+    }
+    uint32_t p = pos[t];
+    for (int z = 0; z < n[2]; ++z)
+      for (int y = 0; y < n[1]; ++y)
+      {
+        // upstream weight order: (K[z] * K[y]) * K[x]
+        const float wzy = g.dim == 3 ? __fmul_rn(w[2][z], w[1][y]) : w[1][y];
+        const uint32_t rowc =
+            ((uint32_t)cell[2][z] * (uint32_t)g.G[1] + (uint32_t)cell[1][y]) *
+            (uint32_t)g.G[0];
+        for (int x = 0; x < n[0]; ++x)
+        {
+          keys[p] = rowc + (uint32_t)cell[0][x];
+          ids[p] = p;
+          pairs[p] = make_uint2((uint32_t)t,
+                                __float_as_uint(__fmul_rn(wzy, w[0][x])));
+          ++p;
+        }
+      }
+  }
+}
+
+__global__ void k_gather_pairs(const uint32_t *__restrict__ ids,
+                               const uint2 *__restrict__ pairs, size_t n,
+                               uint2 *__restrict__ out)
+{
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    out[i] = pairs[ids[i]];
+}
+
 int bits_for(uint32_t max_value)
 {
   int b = 1;
@@ -402,6 +461,54 @@ size_t build_owner_candidates(const float *traj_sorted,
                     cand_offsets.as<uint32_t>(), s);
   GN_CUDA(cudaStreamSynchronize(s));
   return total;
+}
+
+size_t build_interp_matrix(const float *traj_sorted,
+                           const uint32_t *sector_sorted, uint32_t M,
+                           const Geo &g, const float *lut,
+                           DeviceBuffer &row_off, DeviceBuffer &nz,
+                           cudaStream_t s)
+{
+  const uint32_t G = (uint32_t)g.grid_count;
+  row_off.reset((size_t)(G + 1) * sizeof(uint32_t));
+  if (M == 0)
+  {
+    GN_CUDA(cudaMemsetAsync(row_off.get(), 0, (size_t)(G + 1) * 4, s));
+    nz.reset(sizeof(uint2));
+    return 0;
+  }
+  DeviceBuffer count((size_t)(M + 1) * sizeof(uint32_t));
+  GN_CUDA(cudaMemsetAsync(count.get(), 0, (size_t)(M + 1) * 4, s));
+  const unsigned nb = grid_for(M, 256, 8192);
+  k_interp_pairs<false><<<nb, 256, 0, s>>>(traj_sorted, sector_sorted, M, g,
+                                           lut, count.as<uint32_t>(), nullptr,
+                                           nullptr, nullptr, nullptr);
+  GN_LAUNCH_CHECK("interp count");
+  scan_exclusive(count.as<uint32_t>(), count.as<uint32_t>(), (size_t)M + 1,
+                 s);
+  uint32_t total = 0;
+  GN_CUDA(cudaMemcpyAsync(&total, count.as<uint32_t>() + M, sizeof(uint32_t),
+                          cudaMemcpyDeviceToHost, s));
+  GN_CUDA(cudaStreamSynchronize(s));
+  const size_t n = total;
+  DeviceBuffer keys(n * 4 + 4), ids(n * 4 + 4), pairs(n * 8 + 8);
+  k_interp_pairs<true><<<nb, 256, 0, s>>>(
+      traj_sorted, sector_sorted, M, g, lut, nullptr, count.as<uint32_t>(),
+      keys.as<uint32_t>(), ids.as<uint32_t>(), pairs.as<uint2>());
+  GN_LAUNCH_CHECK("interp fill");
+  count.release();
+  DeviceBuffer skeys(n * 4 + 4), sids(n * 4 + 4);
+  sort_pairs(keys.as<uint32_t>(), ids.as<uint32_t>(), skeys.as<uint32_t>(),
+             sids.as<uint32_t>(), n, bits_for(G ? G - 1 : 0), s);
+  keys.release();
+  ids.release();
+  nz.reset(n * 8 + 8);
+  k_gather_pairs<<<grid_for(n, 256, 8192), 256, 0, s>>>(
+      sids.as<uint32_t>(), pairs.as<uint2>(), n, nz.as<uint2>());
+  GN_LAUNCH_CHECK("interp gather");
+  histogram_offsets(skeys.as<uint32_t>(), n, G, row_off.as<uint32_t>(), s);
+  GN_CUDA(cudaStreamSynchronize(s));
+  return n;
 }
 
 }  // namespace gnufft

@@ -48,4 +48,17 @@ size_t build_owner_candidates(const float *traj_sorted,
                               DeviceBuffer &cand, DeviceBuffer &cand_offsets,
                               cudaStream_t s);
 
+// Interpolation matrix of the trajectory in CSR form keyed by grid cell:
+// for every (unshifted, x-fastest) grid cell the list of (sorted sample t,
+// kernel weight) pairs whose footprint covers it, ascending in t.  The
+// weights are the upstream's (K[z] * K[y]) * K[x] (or the texture
+// interpolation), footprints as the upstream kernels compute them.
+// Output: row_off [G + 1] (u32) and nz [nnz] (uint2: t, weight bits).
+// Returns nnz.
+size_t build_interp_matrix(const float *traj_sorted,
+                           const uint32_t *sector_sorted, uint32_t M,
+                           const Geo &g, const float *lut,
+                           DeviceBuffer &row_off, DeviceBuffer &nz,
+                           cudaStream_t s);
+
 }  // namespace gnufft

@@ -242,8 +242,14 @@ __global__ void __launch_bounds__(512)
   int *s_wc = s_cnt + NB;          // [NB][16]
   float2 *s_v = reinterpret_cast<float2 *>(
       reinterpret_cast<uintptr_t>(s_wc + NB * 16 + 3) & ~uintptr_t(15));
-  for (int i = threadIdx.x; i < cells * PITCH; i += nthreads)
-    tile[i] = make_float2(0.f, 0.f);
+  {
+    float4 *t4 = reinterpret_cast<float4 *>(tile);
+    const int n4 = (cells * PITCH) / 2;
+    for (int i = threadIdx.x; i < n4; i += nthreads)
+      t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if ((cells * PITCH) & 1)
+      tile[cells * PITCH - 1] = make_float2(0.f, 0.f);
+  }
   int ta[3];
   split_sector(it.target, g, ta);
 
@@ -318,6 +324,20 @@ __global__ void __launch_bounds__(512)
           s_wc[b * 16 + warp] = __popc(ball);
       }
       __syncthreads();
+      // stage the chunk's k-space rows (this coil group) in shared memory
+      {
+        const int nck = min(CH, it.end - base);
+        constexpr int V4 = CG >= 2 ? CG / 2 : 1;  // 16-byte pieces per row
+        for (int q = threadIdx.x; q < nck * V4; q += nthreads)
+        {
+          const int r = q / V4, k = q - r * V4;
+          const float2 *src = ks + (size_t)s_t[r] * CP + group * CG;
+          if (CG >= 2)
+            cp_async16(s_v + r * CG + 2 * k, src + 2 * k);
+          else
+            cp_async8(s_v + r * CG, src);
+        }
+      }
       if (threadIdx.x < NB)
       {
         const int b = threadIdx.x;
@@ -344,19 +364,6 @@ __global__ void __launch_bounds__(512)
           const int pos = s_wc[b * 16 + warp] + __popc(ball & lt);
           s_list[b * CH + pos] = (unsigned short)((threadIdx.x << 3) | e);
         }
-      }
-      // stage the chunk's k-space rows (this coil group) in shared memory
-      const int nc = min(CH, it.end - base);
-      constexpr int V4 = CG >= 2 ? CG / 2 : 1;  // 16-byte pieces per row
-      __syncthreads();  // s_t of the chunk visible to every thread
-      for (int q = threadIdx.x; q < nc * V4; q += nthreads)
-      {
-        const int r = q / V4, k = q - r * V4;
-        const float2 *src = ks + (size_t)s_t[r] * CP + group * CG;
-        if (CG >= 2)
-          cp_async16(s_v + r * CG + 2 * k, src + 2 * k);
-        else
-          cp_async8(s_v + r * CG, src);
       }
       cp_async_wait_all();
     }
@@ -484,29 +491,143 @@ __global__ void __launch_bounds__(512)
   }
 }
 
+// Zero the owned cells of targets that no spread block writes with plain
+// stores (targets without candidates, and split targets whose blocks add
+// atomically).  One block per target; lanes along x, no divisions per cell.
 template <int DIM>
-__global__ void k_zero_split(const int *__restrict__ targets, Geo g, int C,
-                             int shift, float2 *__restrict__ grid)
+__global__ void k_zero_targets(const int *__restrict__ targets, Geo g, int C,
+                               int shift, float2 *__restrict__ grid)
 {
+  __shared__ long long s_rowoff[kMaxBuckets * kMaxBuckets];
+  __shared__ int s_xoff[kMaxBuckets];
   int ta[3];
   split_sector(targets[blockIdx.x], g, ta);
   const int sw = g.sw;
-  const int cells = DIM == 3 ? sw * sw * sw : sw * sw;
-  for (int i = threadIdx.x; i < cells * C; i += blockDim.x)
+  const int nrows = DIM == 3 ? sw * sw : sw;
+  for (int r = threadIdx.x; r < nrows; r += blockDim.x)
   {
-    const int c = i / cells, cell = i - c * cells;
-    int gx = ta[0] * sw + cell % sw, gy = ta[1] * sw + (cell / sw) % sw;
-    int gz = DIM == 3 ? ta[2] * sw + cell / (sw * sw) : 0;
-    if (gx >= g.G[0] || gy >= g.G[1] || gz >= g.G[2])
-      continue;
-    if (shift)
+    const int y = r % sw, z = DIM == 3 ? r / sw : 0;
+    int gy = ta[1] * sw + y, gz = DIM == 3 ? ta[2] * sw + z : 0;
+    long long off = -1;
+    if (gy < g.G[1] && gz < g.G[2])
     {
-      gx = wrap_mod(gx - g.shift_inv[0], g.G[0]);
-      gy = wrap_mod(gy - g.shift_inv[1], g.G[1]);
-      gz = DIM == 3 ? wrap_mod(gz - g.shift_inv[2], g.G[2]) : 0;
+      if (shift)
+      {
+        gy = wrap_mod(gy - g.shift_inv[1], g.G[1]);
+        gz = DIM == 3 ? wrap_mod(gz - g.shift_inv[2], g.G[2]) : 0;
+      }
+      off = ((long long)gz * g.G[1] + gy) * g.G[0];
     }
-    grid[((long long)gz * g.G[1] + gy) * g.G[0] + gx +
-         (long long)c * g.grid_count] = make_float2(0.f, 0.f);
+    s_rowoff[r] = off;
+  }
+  for (int x = threadIdx.x; x < sw; x += blockDim.x)
+  {
+    const int gx = ta[0] * sw + x;
+    s_xoff[x] = gx < g.G[0] ? (shift ? wrap_mod(gx - g.shift_inv[0], g.G[0])
+                                     : gx)
+                            : -1;
+  }
+  __syncthreads();
+  const int x0 = threadIdx.x % sw;
+  const int rstep = blockDim.x / sw;
+  const int r0 = threadIdx.x / sw;
+  if (r0 >= rstep)
+    return;
+  const int xo = s_xoff[x0];
+  if (xo < 0)
+    return;
+  for (int c = 0; c < C; ++c)
+  {
+    float2 *gc = grid + (long long)c * g.grid_count + xo;
+    for (int r = r0; r < nrows; r += rstep)
+    {
+      const long long ro = s_rowoff[r];
+      if (ro >= 0)
+        gc[ro] = make_float2(0.f, 0.f);
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// adjoint as a product with the interpolation matrix (CSR by grid cell)
+// --------------------------------------------------------------------------
+// One block per (grid row, 64-cell x chunk, coil group).  Each warp slot
+// accumulates whole cells -- all CG coils in its lanes, in registers -- from
+// the cell's (sample, weight) list, reading 8*CG contiguous bytes of the
+// sorted k-space per entry; the chunk is then written once per coil with
+// coalesced stores (INVERSE fftshift folded into the store position).  No
+// atomics, no read-modify-write, fixed summation order.
+constexpr int kSpmmCells = 64;
+
+template <int CG>
+__global__ void __launch_bounds__(kThreads)
+    k_adjoint_spmm(const uint32_t *__restrict__ row_off,
+                   const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
+                   int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
+{
+  constexpr int SLOTS = 32 / CG;
+  __shared__ float2 acc_s[kSpmmCells][CG + 1];
+  const int x0 = blockIdx.y * kSpmmCells;
+  const int row = blockIdx.x;  // y + G1 * z
+  const int group = blockIdx.z;
+  const int nxc = min(kSpmmCells, g.G[0] - x0);
+  const long long rowbase = (long long)row * g.G[0];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = lane / CG, coil = lane % CG;
+  const float2 *ksg = ks + group * CG + coil;
+  for (int i = warp * SLOTS + slot; i < nxc; i += kWarps * SLOTS)
+  {
+    const long long cell = rowbase + x0 + i;
+    const uint32_t b = __ldg(row_off + cell), e = __ldg(row_off + cell + 1);
+    float ax = 0.f, ay = 0.f;
+    uint32_t k = b;
+    for (; k + 4 <= e; k += 4)
+    {
+      uint2 q[4];
+      float2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        q[u] = __ldg(nz + k + u);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        v[u] = __ldg(ksg + (size_t)q[u].x * CP);
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+      {
+        const float w = __uint_as_float(q[u].y);
+        ax = __fmaf_rn(w, v[u].x, ax);
+        ay = __fmaf_rn(w, v[u].y, ay);
+      }
+    }
+    for (; k < e; ++k)
+    {
+      const uint2 q = __ldg(nz + k);
+      const float2 v = __ldg(ksg + (size_t)q.x * CP);
+      const float w = __uint_as_float(q.y);
+      ax = __fmaf_rn(w, v.x, ax);
+      ay = __fmaf_rn(w, v.y, ay);
+    }
+    acc_s[i][coil] = make_float2(ax, ay);
+  }
+  __syncthreads();
+  // store: row and chunk positions after the optional INVERSE fftshift
+  int y = row % g.G[1], z = row / g.G[1];
+  if (shift)
+  {
+    y = wrap_mod(y - g.shift_inv[1], g.G[1]);
+    z = wrap_mod(z - g.shift_inv[2], g.G[2]);
+  }
+  const long long orow = ((long long)z * g.G[1] + y) * g.G[0];
+  for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
+  {
+    const int cl = idx / kSpmmCells, xi = idx - cl * kSpmmCells;
+    const int c = group * CG + cl;
+    if (xi >= nxc || c >= C)
+      continue;
+    int x = x0 + xi;
+    if (shift)
+      x = wrap_mod(x - g.shift_inv[0], g.G[0]);
+    grid[(long long)c * g.grid_count + orow + x] = acc_s[xi][cl];
   }
 }
 
@@ -856,8 +977,8 @@ void adj_dispatch(const AdjItem *items, int n_items, const uint32_t *cand,
                   uint32_t M, int C, bool shift, float2 *grid, cudaStream_t s)
 {
   const int threads = adjoint_block_threads(g, CG);
-  int ch = threads;
-  while (ch > 32 && adjoint_smem_bytes(g, CG, ch) > 220 * 1024)
+  int ch = threads < 128 ? threads : 128;
+  while (ch > 32 && adjoint_smem_bytes(g, CG, ch) > 110 * 1024)
     ch >>= 1;
   const size_t smem = adjoint_smem_bytes(g, CG, ch);
   auto k = k_adjoint_spread<DIM, CG, KS>;
@@ -895,7 +1016,34 @@ int pow2_at_least(int c)
 int slots_for(const Geo &g) { return g.kw + 1 <= 4 ? 4 : 8; }
 }  // namespace
 
-int adjoint_coil_group(int C) { return C > 16 ? 32 : pow2_at_least(C); }
+// 16 coil lanes per group for larger coil counts: two resident blocks per
+// SM (the 32-lane tile alone takes ~135 KB of shared memory in 3-D); fewer
+// lanes when the sector tile is large.
+int adjoint_coil_group(int C, const Geo &g)
+{
+  int cg = C > 8 ? 16 : pow2_at_least(C);
+  while (cg > 1 && adjoint_smem_bytes(g, cg, 32) > 200 * 1024)
+    cg >>= 1;
+  return cg;
+}
+
+int spmm_coil_group(int C) { return C > 16 ? 32 : pow2_at_least(C); }
+
+bool gridding_supported(const Geo &g, std::string &why)
+{
+  if (g.sw > kMaxBuckets)
+  {
+    why = "sector width above 32 is not supported";
+    return false;
+  }
+  if (adjoint_smem_bytes(g, 1, 32) > 200 * 1024 ||
+      forward_smem_bytes(g, 1) > 200 * 1024)
+  {
+    why = "sector tile exceeds shared memory (3-D sector width too large)";
+    return false;
+  }
+  return true;
+}
 
 int forward_coil_group(int C, int dim, int pad)
 {
@@ -960,13 +1108,15 @@ void launch_zero_split(const int *targets, int n_targets, const Geo &g, int C,
 {
   if (n_targets <= 0)
     return;
+  if (g.sw > kMaxBuckets)
+    throw Error(kNotSupported, "sector width above 32");
   if (g.dim == 3)
-    k_zero_split<3><<<n_targets, kThreads, 0, s>>>(targets, g, C, shift,
-                                                   grid);
+    k_zero_targets<3><<<n_targets, kThreads, 0, s>>>(targets, g, C, shift,
+                                                     grid);
   else
-    k_zero_split<2><<<n_targets, kThreads, 0, s>>>(targets, g, C, shift,
-                                                   grid);
-  GN_LAUNCH_CHECK("zero split targets");
+    k_zero_targets<2><<<n_targets, kThreads, 0, s>>>(targets, g, C, shift,
+                                                     grid);
+  GN_LAUNCH_CHECK("zero targets");
 }
 
 void launch_adjoint_spread(const AdjItem *items, int n_items,
@@ -977,7 +1127,7 @@ void launch_adjoint_spread(const AdjItem *items, int n_items,
 {
   if (n_items <= 0)
     return;
-  const int cg = adjoint_coil_group(C);
+  const int cg = adjoint_coil_group(C, g);
 #define GN_ADJ(D, CGV)                                                         \
   if (slots_for(g) == 4)                                                       \
     adj_dispatch<D, CGV, 4>(items, n_items, cand, sector_sorted, traj_sorted, \
@@ -1005,6 +1155,29 @@ void launch_adjoint_spread(const AdjItem *items, int n_items,
   }
 #undef GN_ADJ_CG
 #undef GN_ADJ
+}
+
+void launch_adjoint_spmm(const uint32_t *row_off, const uint2 *nz,
+                         const float2 *ks, int CP, const Geo &g, int C,
+                         bool shift, float2 *grid, cudaStream_t s)
+{
+  const int cg = spmm_coil_group(C);
+  dim3 grd(g.G[1] * g.G[2], (g.G[0] + kSpmmCells - 1) / kSpmmCells,
+           (C + cg - 1) / cg);
+#define GN_SPMM(CGV)                                                           \
+  k_adjoint_spmm<CGV><<<grd, kThreads, 0, s>>>(row_off, nz, ks, CP, g, C,     \
+                                               shift ? 1 : 0, grid)
+  switch (cg)
+  {
+  case 1: GN_SPMM(1); break;
+  case 2: GN_SPMM(2); break;
+  case 4: GN_SPMM(4); break;
+  case 8: GN_SPMM(8); break;
+  case 16: GN_SPMM(16); break;
+  default: GN_SPMM(32); break;
+  }
+#undef GN_SPMM
+  GN_LAUNCH_CHECK("adjoint spmm");
 }
 
 void launch_adjoint_finish(const float2 *grid, const float *deapo,

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 
 #include <cuda_runtime.h>
 
@@ -31,7 +32,9 @@ struct FwdItem
 };
 
 // Coil-group width used by the spread / interpolation kernels for C coils.
-int adjoint_coil_group(int C);
+int adjoint_coil_group(int C, const Geo &g);
+// Whether the sector tiles of this geometry fit the kernels (why if not).
+bool gridding_supported(const Geo &g, std::string &why);
 int forward_coil_group(int C, int dim, int pad);
 
 // Launch shape / dynamic shared memory of the kernels.
@@ -58,6 +61,17 @@ void launch_adjoint_spread(const AdjItem *items, int n_items,
                            const float *traj_sorted, const float2 *ks, int CP,
                            const Geo &g, const float *lut, uint32_t M, int C,
                            bool shift, float2 *grid, cudaStream_t s);
+
+// Coil-group width of the sparse adjoint (lanes per cell).
+int spmm_coil_group(int C);
+
+// Adjoint spread as a product with the interpolation matrix (CSR by grid
+// cell): grid [C][G] = W * ks, every cell written once.  With `shift`, cell
+// g is stored at (g - floor(G/2)) mod G per axis (the upstream's INVERSE
+// fftshift ahead of the inverse FFT).  ks: [M][CP] sorted k-space.
+void launch_adjoint_spmm(const uint32_t *row_off, const uint2 *nz,
+                         const float2 *ks, int CP, const Geo &g, int C,
+                         bool shift, float2 *grid, cudaStream_t s);
 
 // Adjoint finish: crop of the (shifted) inverse-FFT output, 1/sqrt(Ng),
 // deapodization, conj(sens) multiply and coil sum.  stage: 1 = FFT (crop +

@@ -76,6 +76,8 @@ struct gnufft_plan
   // resident device tables
   DeviceBuffer lut, traj_sorted, di, sec_sorted, dens_sorted, cand, cand_off;
   DeviceBuffer adj_items, split_targets, fwd_items, deapo, sens;
+  DeviceBuffer w_rows, w_nz;  // interpolation matrix, CSR by grid cell
+  size_t nnz = 0;
   int n_adj_items = 0, n_split = 0, n_fwd_items = 0;
   size_t n_cand = 0;
   uint32_t sens_coils = 0;
@@ -115,6 +117,7 @@ struct gnufft_plan
                                   &sec_sorted,  &dens_sorted, &cand,
                                   &cand_off,    &adj_items,   &split_targets,
                                   &fwd_items,   &deapo,       &sens,
+                                  &w_rows,      &w_nz,
                                   &ks,          &grid,        &stage_in,
                                   &stage_out,   &one_sens};
     size_t s = 0;
@@ -274,36 +277,9 @@ void sector_centers(const Geo &g, std::vector<uint32_t> &c)
       }
 }
 
-void build_items(gnufft_plan &p, const std::vector<uint32_t> &cand_off)
+void build_items(gnufft_plan &p)
 {
   const int S = p.g.n_sectors;
-  std::vector<AdjItem> split, single;
-  std::vector<int> split_t;
-  for (int t = 0; t < S; ++t)
-  {
-    const uint32_t b = cand_off[t], e = cand_off[t + 1];
-    const uint32_t n = e - b;
-    if (n <= (uint32_t)kAdjPayload)
-    {
-      single.push_back(AdjItem{t, (int)b, (int)e, 0});
-      continue;
-    }
-    split_t.push_back(t);
-    for (uint32_t s = b; s < e; s += kAdjPayload)
-      split.push_back(
-          AdjItem{t, (int)s, (int)std::min<uint32_t>(e, s + kAdjPayload), 1});
-  }
-  std::stable_sort(split.begin(), split.end(),
-                   [](const AdjItem &a, const AdjItem &b) {
-                     return (a.end - a.begin) > (b.end - b.begin);
-                   });
-  std::vector<AdjItem> items(split);
-  items.insert(items.end(), single.begin(), single.end());
-  p.n_adj_items = (int)items.size();
-  p.n_split = (int)split_t.size();
-  upload(p.adj_items, items.data(), items.size(), p.stream);
-  upload(p.split_targets, split_t.data(), split_t.size(), p.stream);
-
   std::vector<FwdItem> fitems;
   for (int s = 0; s < S; ++s)
   {
@@ -331,6 +307,8 @@ void init_common(gnufft_plan &p, const gnufft_desc *d)
   if (!make_geo(d->img_dims, d->osf, d->kernel_width, d->sector_width,
                 p.texture, p.g, err))
     throw Error(kInvalidArgument, err);
+  if (!gridding_supported(p.g, err))
+    throw Error(kNotSupported, err);
   p.dim = p.g.dim;
   p.M = d->n_samples;
   if ((size_t)p.M * (p.dim + 2) >= (1ull << 31))
@@ -361,15 +339,11 @@ void set_sens_host(gnufft_plan &p, const void *sens, uint32_t n_coils)
 
 void finish_tables(gnufft_plan &p)
 {
-  // owner candidates and work items
-  build_owner_candidates(p.traj_sorted.as<float>(), p.sec_sorted.as<uint32_t>(),
-                         p.M, p.g, p.lut.as<float>(), p.cand, p.cand_off,
-                         p.stream);
-  std::vector<uint32_t> cand_off_h;
-  download(cand_off_h, p.cand_off, (size_t)p.g.n_sectors + 1, p.stream);
-  GN_CUDA(cudaStreamSynchronize(p.stream));
-  p.n_cand = cand_off_h.back();
-  build_items(p, cand_off_h);
+  // interpolation matrix (adjoint) and forward work items
+  p.nnz = build_interp_matrix(p.traj_sorted.as<float>(),
+                              p.sec_sorted.as<uint32_t>(), p.M, p.g,
+                              p.lut.as<float>(), p.w_rows, p.w_nz, p.stream);
+  build_items(p);
   processing_order(p.sdc_h, p.order_h);
   upload(p.deapo, p.deapo_h.data(), p.deapo_h.size(), p.stream);
   GN_CUDA(cudaStreamSynchronize(p.stream));
@@ -521,7 +495,7 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
                      bool accumulate = false)
 {
   const Geo &g = p.g;
-  const int cg = adjoint_coil_group((int)C);
+  const int cg = spmm_coil_group((int)C);
   const int CP = ((int)C + cg - 1) / cg * cg;
   p.ks.ensure((size_t)p.M * CP * sizeof(float2));
   const bool conv = stage == GNUFFT_CONVOLUTION ||
@@ -539,16 +513,8 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
   p.launches += 1;
   p.mark(1, s);
   p.mark(2, s);
-  if (p.n_split)
-  {
-    launch_zero_split(p.split_targets.as<int>(), p.n_split, g, (int)C, !conv,
-                      grid, s);
-    p.launches += 1;
-  }
-  launch_adjoint_spread(p.adj_items.as<AdjItem>(), p.n_adj_items,
-                        p.cand.as<uint32_t>(), p.sec_sorted.as<uint32_t>(),
-                        p.traj_sorted.as<float>(), p.ks.as<float2>(), CP, g,
-                        p.lut.as<float>(), p.M, (int)C, !conv, grid, s);
+  launch_adjoint_spmm(p.w_rows.as<uint32_t>(), p.w_nz.as<uint2>(),
+                      p.ks.as<float2>(), CP, g, (int)C, !conv, grid, s);
   p.launches += 1;
   p.mark(3, s);
   p.mark(4, s);
