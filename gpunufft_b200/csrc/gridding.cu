@@ -566,51 +566,20 @@ __global__ void __launch_bounds__(kThreads)
                    int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
 {
   constexpr int SLOTS = 32 / CG;
+  constexpr int NU = kWarps * SLOTS;  // streaming units per block
+  constexpr int B = 8;                // entries per batch
   __shared__ float2 acc_s[kSpmmCells][CG + 1];
+  __shared__ uint32_t s_off[kSpmmCells + 1];
   const int x0 = blockIdx.y * kSpmmCells;
   const int row = blockIdx.x;  // y + G1 * z
   const int group = blockIdx.z;
   const int nxc = min(kSpmmCells, g.G[0] - x0);
-  const long long rowbase = (long long)row * g.G[0];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slot = lane / CG, coil = lane % CG;
-  const float2 *ksg = ks + group * CG + coil;
-  for (int i = warp * SLOTS + slot; i < nxc; i += kWarps * SLOTS)
-  {
-    const long long cell = rowbase + x0 + i;
-    const uint32_t b = __ldg(row_off + cell), e = __ldg(row_off + cell + 1);
-    float ax = 0.f, ay = 0.f;
-    uint32_t k = b;
-    for (; k + 4 <= e; k += 4)
-    {
-      uint2 q[4];
-      float2 v[4];
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        q[u] = __ldg(nz + k + u);
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-        v[u] = __ldg(ksg + (size_t)q[u].x * CP);
-#pragma unroll
-      for (int u = 0; u < 4; ++u)
-      {
-        const float w = __uint_as_float(q[u].y);
-        ax = __fmaf_rn(w, v[u].x, ax);
-        ay = __fmaf_rn(w, v[u].y, ay);
-      }
-    }
-    for (; k < e; ++k)
-    {
-      const uint2 q = __ldg(nz + k);
-      const float2 v = __ldg(ksg + (size_t)q.x * CP);
-      const float w = __uint_as_float(q.y);
-      ax = __fmaf_rn(w, v.x, ax);
-      ay = __fmaf_rn(w, v.y, ay);
-    }
-    acc_s[i][coil] = make_float2(ax, ay);
-  }
+  const long long rowbase = (long long)row * g.G[0] + x0;
+  for (int i = threadIdx.x; i <= nxc; i += kThreads)
+    s_off[i] = __ldg(row_off + rowbase + i);
   __syncthreads();
-  // store: row and chunk positions after the optional INVERSE fftshift
+  const uint32_t A = s_off[0], E = s_off[nxc];
+  // output row after the optional INVERSE fftshift
   int y = row % g.G[1], z = row / g.G[1];
   if (shift)
   {
@@ -618,6 +587,92 @@ __global__ void __launch_bounds__(kThreads)
     z = wrap_mod(z - g.shift_inv[2], g.G[2]);
   }
   const long long orow = ((long long)z * g.G[1] + y) * g.G[0];
+  if (A == E)
+  {  // no sample reaches these cells: plain zero stores
+    for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
+    {
+      const int cl = idx / kSpmmCells, xi = idx - cl * kSpmmCells;
+      const int c = group * CG + cl;
+      if (xi >= nxc || c >= C)
+        continue;
+      int x = x0 + xi;
+      if (shift)
+        x = wrap_mod(x - g.shift_inv[0], g.G[0]);
+      grid[(long long)c * g.grid_count + orow + x] = make_float2(0.f, 0.f);
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < kSpmmCells * (CG + 1); i += kThreads)
+    (&acc_s[0][0])[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int slot = lane / CG, coil = lane % CG;
+  const int unit = warp * SLOTS + slot;
+  const float2 *ksg = ks + group * CG + coil;
+  // an equal share of the block's contiguous nonzero range per unit
+  const uint32_t len = (E - A + NU - 1) / NU;
+  const uint32_t u0 = min(E, A + unit * len), u1 = min(E, u0 + len);
+  // first cell whose range contains u0: count the bounds <= u0 with the
+  // CG lanes of this slot (uniform trip count across the warp)
+  int cell = 0;
+  const unsigned slot_bits =
+      (CG == 32 ? 0xffffffffu : ((1u << CG) - 1u)) << (slot * CG);
+  for (int base = 0; base < nxc; base += CG)
+  {
+    const int i = base + coil + 1;
+    const bool le = i <= nxc && s_off[i] <= u0;
+    cell += __popc(__ballot_sync(0xffffffffu, le) & slot_bits);
+  }
+  if (u0 < u1)
+  {
+    uint32_t bound = s_off[cell + 1];
+    float ax = 0.f, ay = 0.f;
+    uint2 qn[B];
+#pragma unroll
+    for (int u = 0; u < B; ++u)
+      qn[u] = (u0 + u < u1) ? __ldg(nz + u0 + u) : make_uint2(0u, 0u);
+    for (uint32_t k0 = u0; k0 < u1; k0 += B)
+    {
+      uint2 q[B];
+#pragma unroll
+      for (int u = 0; u < B; ++u)
+        q[u] = qn[u];
+      const bool full = k0 + B <= u1;
+      // prefetch the next batch of (sample, weight) pairs
+#pragma unroll
+      for (int u = 0; u < B; ++u)
+        qn[u] = (k0 + B + u < u1) ? __ldg(nz + k0 + B + u)
+                                  : make_uint2(0u, 0u);
+      float2 v[B];
+#pragma unroll
+      for (int u = 0; u < B; ++u)
+        v[u] = (full || k0 + u < u1) ? __ldg(ksg + (size_t)q[u].x * CP)
+                                     : make_float2(0.f, 0.f);
+      const uint32_t nb = full ? B : u1 - k0;
+#pragma unroll
+      for (int u = 0; u < B; ++u)
+      {
+        if ((uint32_t)u >= nb)
+          break;
+        const uint32_t k = k0 + u;
+        while (k >= bound)
+        {  // cell boundary: flush the running sum
+          atomicAdd(&acc_s[cell][coil].x, ax);
+          atomicAdd(&acc_s[cell][coil].y, ay);
+          ax = ay = 0.f;
+          ++cell;
+          bound = s_off[cell + 1];
+        }
+        const float w = __uint_as_float(q[u].y);
+        ax = __fmaf_rn(w, v[u].x, ax);
+        ay = __fmaf_rn(w, v[u].y, ay);
+      }
+    }
+    atomicAdd(&acc_s[cell][coil].x, ax);
+    atomicAdd(&acc_s[cell][coil].y, ay);
+  }
+  __syncthreads();
   for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
   {
     const int cl = idx / kSpmmCells, xi = idx - cl * kSpmmCells;
@@ -885,9 +940,33 @@ __global__ void k_adjoint_finish(const float2 *__restrict__ grid,
   }
 }
 
-// One block per grid row (coil, z, y); threads along x.  Rows whose
-// (shifted) position falls outside the zero-padded image are pure zero
-// stores.
+// Each block handles grid rows (coil, z, y) with threads along x, two
+// cells per thread (16-byte stores).  Rows whose (shifted) position falls
+// outside the zero-padded image are pure zero stores.
+template <bool SENS>
+__device__ __forceinline__ float2 prepare_value(const float2 *__restrict__ image,
+                                                const float2 *__restrict__ sens,
+                                                const float *__restrict__ deapo,
+                                                long long p, long long cN)
+{
+  float2 v;
+  if (SENS)
+  {  // sensMulKernel (std_gpuNUFFT_kernels.cu:142-156)
+    const float2 a = __ldg(image + p);
+    const float2 s = __ldg(sens + p + cN);
+    v.x = a.x * s.x - a.y * s.y;
+    v.y = a.x * s.y + a.y * s.x;
+  }
+  else
+  {
+    v = __ldg(image + p + cN);
+  }
+  const float d = __ldg(deapo + p);
+  v.x = __fmul_rn(v.x, d);
+  v.y = __fmul_rn(v.y, d);
+  return v;
+}
+
 template <bool SENS>
 __global__ void __launch_bounds__(kThreads)
     k_forward_prepare(const float2 *__restrict__ image,
@@ -901,7 +980,17 @@ __global__ void __launch_bounds__(kThreads)
   const long long N = g.img_count;
   const long long plane = (long long)X * Y * Z;
   const long long rows = (long long)Y * Z * C;
-  for (long long r = blockIdx.x; r < rows; r += gridDim.x)
+  const int X2 = X >> 1;  // cell pairs per row
+  const bool vec = (X & 1) == 0;
+  // threads per row: one 16-byte store each (or one cell for odd rows)
+  const int work = vec ? X2 : X;
+  const int tpr = work >= kThreads ? kThreads : (work > 0 ? work : 1);
+  const int rpb = kThreads / tpr;  // rows per block pass
+  const int lr = threadIdx.x / tpr, lt = threadIdx.x - lr * tpr;
+  if (lr >= rpb)
+    return;
+  for (long long r = (long long)blockIdx.x * rpb + lr; r < rows;
+       r += (long long)gridDim.x * rpb)
   {
     const int y = (int)(r % Y);
     const long long rz = r / Y;
@@ -916,47 +1005,58 @@ __global__ void __launch_bounds__(kThreads)
       pz = wrap_mod(z + g.shift_inv[2], g.G[2]) - g.crop[2];
     }
     const bool row_in = py >= 0 && py < g.N[1] && pz >= 0 && pz < g.N[2];
-    if (!row_in)
-    {
-      if ((X & 1) == 0 && ((reinterpret_cast<size_t>(dst) & 15) == 0))
-      {
-        float4 *d4 = reinterpret_cast<float4 *>(dst);
-        for (int x = threadIdx.x; x < X / 2; x += blockDim.x)
-          d4[x] = make_float4(0.f, 0.f, 0.f, 0.f);
-      }
-      else
-      {
-        for (int x = threadIdx.x; x < X; x += blockDim.x)
-          dst[x] = make_float2(0.f, 0.f);
-      }
-      continue;
-    }
     const long long prow = ((long long)pz * g.N[1] + py) * g.N[0];
-    for (int x = threadIdx.x; x < X; x += blockDim.x)
+    const long long cN = (long long)c * N;
+    if (vec)
     {
-      const int px = image_grid ? x
-                                : wrap_mod(x + g.shift_inv[0], g.G[0]) -
-                                      g.crop[0];
-      float2 v = make_float2(0.f, 0.f);
-      if (px >= 0 && px < g.N[0])
+      // even rows start on even cells: 16-byte aligned pairs
+      float4 *d4 = reinterpret_cast<float4 *>(dst);
+      for (int j = lt; j < X2; j += tpr)
       {
-        const long long p = prow + px;
-        if (SENS)
-        {  // sensMulKernel (std_gpuNUFFT_kernels.cu:142-156)
-          const float2 a = image[p];
-          const float2 s = sens[p + (long long)c * N];
-          v.x = a.x * s.x - a.y * s.y;
-          v.y = a.x * s.y + a.y * s.x;
-        }
-        else
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (row_in)
         {
-          v = image[p + (long long)c * N];
+          const int xa = 2 * j;
+          const int pa = image_grid ? xa
+                                    : wrap_mod(xa + g.shift_inv[0], g.G[0]) -
+                                          g.crop[0];
+          const int pb = image_grid ? xa + 1
+                                    : wrap_mod(xa + 1 + g.shift_inv[0],
+                                               g.G[0]) -
+                                          g.crop[0];
+          if (pa >= 0 && pa < g.N[0])
+          {
+            const float2 v = prepare_value<SENS>(image, sens, deapo, prow + pa,
+                                                 cN);
+            o.x = v.x;
+            o.y = v.y;
+          }
+          if (pb >= 0 && pb < g.N[0])
+          {
+            const float2 v = prepare_value<SENS>(image, sens, deapo, prow + pb,
+                                                 cN);
+            o.z = v.x;
+            o.w = v.y;
+          }
         }
-        const float d = deapo[p];
-        v.x = __fmul_rn(v.x, d);
-        v.y = __fmul_rn(v.y, d);
+        d4[j] = o;
       }
-      dst[x] = v;
+    }
+    else
+    {
+      for (int x = lt; x < X; x += tpr)
+      {
+        float2 v = make_float2(0.f, 0.f);
+        if (row_in)
+        {
+          const int px = image_grid ? x
+                                    : wrap_mod(x + g.shift_inv[0], g.G[0]) -
+                                          g.crop[0];
+          if (px >= 0 && px < g.N[0])
+            v = prepare_value<SENS>(image, sens, deapo, prow + px, cN);
+        }
+        dst[x] = v;
+      }
     }
   }
 }
@@ -1201,7 +1301,7 @@ void launch_forward_prepare(const float2 *image, const float2 *sens,
 {
   const size_t rows = (size_t)C * (image_grid ? (size_t)g.N[1] * g.N[2]
                                               : (size_t)g.G[1] * g.G[2]);
-  const unsigned nb = (unsigned)std::min<size_t>(rows, 148 * 64);
+  const unsigned nb = (unsigned)std::min<size_t>(rows, 148 * 32);
   if (sens)
     k_forward_prepare<true><<<nb, kThreads, 0, s>>>(image, sens, deapo, g, C,
                                                     image_grid, grid);
