@@ -32,6 +32,7 @@ EXPORTED = (
     "gnufft_adjoint_host", "gnufft_adjoint_device", "gnufft_forward_host",
     "gnufft_forward_device", "gnufft_set_timing", "gnufft_get_stage_times",
     "gnufft_last_error", "gnufft_status_string", "gnufft_version",
+    "gnufft_adjoint_convolution_noalloc",
 )
 
 
@@ -116,6 +117,8 @@ def lib() -> ctypes.CDLL:
         f = getattr(L, name)
         f.restype = st
         f.argtypes = [_P, _P, _P, _U, _I, _P]
+    L.gnufft_adjoint_convolution_noalloc.restype = st
+    L.gnufft_adjoint_convolution_noalloc.argtypes = [_P, _P, _P, _U, _P]
     L.gnufft_set_timing.restype = st
     L.gnufft_set_timing.argtypes = [_P, ctypes.c_int]
     L.gnufft_get_stage_times.restype = st

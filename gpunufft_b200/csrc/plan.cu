@@ -28,6 +28,7 @@
 #include "footprint.cuh"
 #include "geometry.hpp"
 #include "gridding.cuh"
+#include "planview.hpp"
 
 using namespace gnufft;
 
@@ -666,6 +667,26 @@ void adjoint_plain(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
 // ==========================================================================
 // C ABI
 // ==========================================================================
+namespace gnufft
+{
+bool plan_view(const gnufft_plan *p, PlanView *v)
+{
+  if (!p || !v)
+    return false;
+  v->g = p->g;
+  v->M = p->M;
+  v->device = p->desc.device;
+  v->sens_coils = p->sens_coils;
+  v->data_indices = p->di.as<uint32_t>();
+  v->dens_sorted = p->has_dens ? p->dens_sorted.as<float>() : nullptr;
+  v->w_rows = p->w_rows.as<uint32_t>();
+  v->w_nz = p->w_nz.as<uint2>();
+  return true;
+}
+
+void set_last_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace gnufft
+
 extern "C" {
 
 const char *gnufft_version(void) { return kVersion; }

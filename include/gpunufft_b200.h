@@ -198,6 +198,30 @@ GNUFFT_API gnufft_status gnufft_forward_device(gnufft_plan *plan, const void *im
                                     void *kspace, uint32_t n_coils,
                                     int32_t output, void *stream);
 
+/* Adjoint up to the CONVOLUTION stage -- the raw oversampled grid
+ * [n_coils][grid], as gnufft_adjoint_device with GNUFFT_CONVOLUTION -- that
+ * performs no device allocation of any kind.  No counterpart in the
+ * upstream library.  It is for callers that may not allocate while they
+ * run: real-time reconstruction loops and serving workers that reserve all
+ * memory up front, code living inside another framework's fixed memory
+ * budget, and callers that cannot afford the device synchronisation that
+ * cudaMalloc / cudaFree imply.  The regular entry points grow the plan's
+ * scratch on first use; this one stages the sorted k-space in a fixed
+ * device array of GNUFFT_NOALLOC_SCRATCH_BYTES inside the library (held on
+ * every GPU that loads the library until the process exits), so
+ * n_samples x coil lanes x 8 bytes must fit in it (coil lanes: n_coils
+ * rounded up to 1, 2, 4, 8, 16 or a multiple of 32); larger requests are
+ * rejected with GNUFFT_ERROR_INVALID_ARGUMENT.  kspace and grid are device
+ * buffers; the call is ordered on `stream`.  The first call on a device
+ * looks up the array's device address (set-up, once per device); make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: calls that overlap on the GPU race and must be serialised by the
+ * caller. */
+#define GNUFFT_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
+GNUFFT_API gnufft_status gnufft_adjoint_convolution_noalloc(
+    gnufft_plan *plan, const void *kspace, void *grid, uint32_t n_coils,
+    void *stream);
+
 /* Device time (ms) of the stages of the last call on this plan, measured
  * with CUDA events when timing is enabled (gnufft_set_timing). */
 typedef struct gnufft_stage_times {
