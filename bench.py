@@ -191,9 +191,9 @@ def cpu_reference(inp, threads, coils_per_step=None):
         ref.cpu_gridding(data[i], crds, lut, t.sector_data_count, t.centers,
                          sw, kw, g.grid[0], grids[i])
 
-    def step():
+    def step(n=threads):
         ths = [threading.Thread(target=one, args=(i,)) for i in
-               range(threads)]
+               range(n)]
         t0 = time.perf_counter()
         for th in ths:
             th.start()
@@ -241,6 +241,33 @@ def run_reference_arm(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def reference_gpu(inp, steps):
+    """fwd+adj/s of the upstream GPU operator (BALANCED, textures off) on
+    this workload, host arrays in and out like its API; None fields when the
+    upstream build is absent."""
+    from oracle import ref
+    note = ("upstream BALANCED operator built from its sources for sm_100a "
+            "(textures off); host arrays per call as its API takes them; "
+            "wall clock")
+    if not ref.available():
+        return {"value": None, "unit": UNIT, "note": note + ": not built"}
+    op = ref.RefGpuOperator(inp["traj"], inp["dims"], inp["C"], inp["kw"],
+                            inp["sw"], inp["osf"], sens=inp["maps"],
+                            balance=True)
+    try:
+        op.forward(inp["x"])
+        op.adjoint(inp["k"])
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            op.forward(inp["x"])
+            op.adjoint(inp["k"])
+        dt = time.perf_counter() - t0
+    finally:
+        op.close()
+    return {"value": steps / dt, "unit": UNIT, "steps": steps,
+            "ms_per_step": dt / steps * 1e3, "note": note}
+
+
 def workload_label(name):
     dims, C, ns, nr, osf, kw, sw = WORKLOADS[name]
     d = "x".join(str(v) for v in dims)
@@ -263,14 +290,14 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def profile_traffic(name):
-    """DRAM bytes per launch of the adjoint spread kernel for this workload
-    from the committed ncu summary, if one exists."""
+def profile_traffic(name, kernel):
+    """DRAM bytes (read + write) per launch of ``kernel`` on workload
+    ``name`` from the committed ncu summary, if one exists."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        return d.get(name, {}).get("adjoint_spread_dram_bytes")
+        return d[name][kernel]["dram_bytes_per_launch"]
     except Exception:
         return None
 
@@ -339,14 +366,27 @@ def run_gpu_arm(args, rank, world, dist):
     g = plan.info
     G_cells = int(np.prod([v for v in g.grid_dims if v]))
     dim = len(dims)
-    spread_ms = avg("adj", "gridding_ms")
-    interp_ms = avg("fwd", "gridding_ms")
-    # algorithmic bytes per launch (k-space read, coordinates, grid write)
-    spread_bytes = 8 * M * C + 4 * dim * M + 8 * G_cells * C
-    interp_bytes = 8 * G_cells * C + 4 * dim * M + 8 * M * C
     peak, src = peaks()
-    achieved = spread_bytes / (spread_ms * 1e-3) / 1e9
-    traffic = profile_traffic(args.workload)
+    # algorithmic bytes per launch of the two gridding kernels: k-space
+    # (8 B per sample per coil), coordinates (4 B per axis per sample) and
+    # the oversampled grid (8 B per cell per coil)
+    gbytes = 8 * M * C + 4 * dim * M + 8 * G_cells * C
+    kernels = {
+        "k_forward_interp": ("forward interpolation", avg("fwd",
+                                                          "gridding_ms")),
+        "k_adjoint_spmm": ("adjoint gridding", avg("adj", "gridding_ms")),
+    }
+    rooflines = []
+    for kname, (what, kms) in kernels.items():
+        ach = gbytes / (kms * 1e-3) / 1e9
+        rooflines.append({
+            "kernel": kname, "what": what, "bound": "hbm", "achieved": ach,
+            "peak": peak, "peak_source": src, "unit": "GB/s",
+            "frac": ach / peak, "traffic": profile_traffic(args.workload,
+                                                           kname),
+            "algorithmic_bytes": gbytes, "launch_ms": kms})
+    # the dominant one of this library's kernels (longest per step)
+    roofline = max(rooflines, key=lambda r: r["launch_ms"])
 
     # end-to-end through the public API: pinned host inputs -> device,
     # fwd + adj, results -> pinned host, every step
@@ -403,6 +443,14 @@ def run_gpu_arm(args, rank, world, dist):
             dist.all_reduce(t, op=dist.ReduceOp.MIN)
             plain_value = float(t.item()) * world
 
+    # the upstream library's own GPU operator, built from its sources for
+    # sm_100a (oracle/_ref), on the same inputs through its host-array API
+    # (performForwardGpuNUFFT / performGpuNUFFTAdj: per-call device
+    # allocation and copies, one coil per pass in 3D); wall clock per step
+    ref_gpu = None
+    if args.ref_gpu_steps > 0:
+        ref_gpu = reference_gpu(inp, args.ref_gpu_steps)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -411,12 +459,17 @@ def run_gpu_arm(args, rank, world, dist):
             step_cpu()
             tcpu = statistics.mean(step_cpu() for _ in range(2))
             cpu_val = threads / (tcpu * 2 * C)
+            t1 = step_cpu(1)
             cpu = {"value": cpu_val, "unit": UNIT, "cores": threads,
                    "kind": "reference",
+                   "single_core_value": 1.0 / (t1 * 2 * C),
+                   "host_threads": cpu_threads(),
                    "sample": (f"upstream gpuNUFFT_cpu adjoint gridding, "
                               f"{threads} coil(s) x 2 steps on {threads} "
-                              f"thread(s); fwd+adj/s = coils/s / (2 x {C}); "
-                              f"FFT and deapodization not counted")}
+                              f"thread(s), one coil per thread; fwd+adj/s = "
+                              f"coils/s / (2 x {C}); FFT and deapodization "
+                              f"not counted; single_core_value: one coil on "
+                              f"one thread")}
         except Exception as e:  # oracle/_ref absent on this machine
             cpu = {"value": None, "unit": UNIT, "cores": 0,
                    "kind": "reference", "sample": f"unavailable: {e}"}
@@ -432,12 +485,8 @@ def run_gpu_arm(args, rank, world, dist):
             "config": {"workload": workload_label(args.workload),
                        "parallelism": f"replicas x{world}",
                        "l2": "inputs and grids larger than L2 (126 MB)"},
-            "roofline": {"kernel": "adjoint spread (k_adjoint_spread)",
-                         "bound": "hbm", "achieved": achieved, "peak": peak,
-                         "peak_source": src, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
-                         "algorithmic_bytes": spread_bytes,
-                         "launch_ms": spread_ms},
+            "roofline": roofline,
+            "rooflines": rooflines,
             "stages_ms": {
                 "forward": {k: avg("fwd", k) for k in
                             ("prepare_ms", "gridding_ms", "fft_ms",
@@ -445,12 +494,12 @@ def run_gpu_arm(args, rank, world, dist):
                 "adjoint": {k: avg("adj", k) for k in
                             ("prepare_ms", "gridding_ms", "fft_ms",
                              "finish_ms")},
-                "forward_interp_gbs": interp_bytes / (interp_ms * 1e-3) / 1e9,
             },
             "plain": {"value": plain_value, "unit": UNIT,
                       "steps": args.plain_steps,
                       "batched_over_plain": (value / plain_value
                                              if plain_value else None)},
+            "reference_gpu": ref_gpu,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -470,6 +519,8 @@ def main():
     ap.add_argument("--workload", default="3d128x32", choices=list(WORKLOADS))
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-gpu-steps", type=int, default=2,
+                    help="steps of the upstream GPU operator (0: skip)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -11,6 +11,7 @@
 // Calls restate GpuNUFFTOperator::performGpuNUFFTAdj / performForwardGpuNUFFT
 // (gpuNUFFT_operator.cpp:370-1294) with all coils of a call in one pass.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -454,14 +455,31 @@ void load_plan(gnufft_plan &p, const gnufft_desc *d, const float *traj_sorted,
   sector_centers(p.g, my_centers);
   if (!std::equal(my_centers.begin(), my_centers.end(), centers))
     throw Error(kInvalidArgument, "sector centers do not match the geometry");
+  // every sorted sample must lie in the sector whose range holds it (the
+  // kernels place a sample's footprint inside its own sector's tile)
+  std::vector<uint32_t> ss(M);
+  for (uint32_t sct = 0; sct < S; ++sct)
+    for (uint32_t t = sdc[sct]; t < sdc[sct + 1]; ++t)
+    {
+      uint32_t id = 0, stride = 1;
+      for (int a = 0; a < dim; ++a)
+      {
+        const float c = traj_sorted[(size_t)a * M + t];
+        if (!std::isfinite(c))
+          throw Error(kInvalidArgument, "trajectory coordinate not finite");
+        id += host_sector_of(c, p.g.G[a], p.g.sw) * stride;
+        stride *= (uint32_t)p.g.S[a];
+      }
+      if (id != sct)
+        throw Error(kInvalidArgument,
+                    "sorted sample " + std::to_string(t) +
+                        " does not lie in sector " + std::to_string(sct));
+      ss[t] = sct;
+    }
   p.sdc_h.assign(sdc, sdc + S + 1);
   p.di_h.assign(di, di + M);
   p.traj_sorted_h.assign(traj_sorted, traj_sorted + (size_t)dim * M);
   p.deapo_h.assign(deapo, deapo + p.g.img_count);
-  std::vector<uint32_t> ss(M);
-  for (uint32_t sct = 0; sct < S; ++sct)
-    for (uint32_t t = sdc[sct]; t < sdc[sct + 1]; ++t)
-      ss[t] = sct;
   cudaStream_t s = p.stream;
   upload(p.di, di, M, s);
   upload(p.sec_sorted, ss.data(), M, s);

@@ -90,6 +90,10 @@ class Plan:
         d.device = int(device)
         self.device = int(device)
         self.n_sens = n_sens
+        self.kernel_width = int(kernel_width)
+        self.sector_width = int(sector_width)
+        self.osf = float(osf)
+        self.operator_type = int(operator_type)
         L = C.lib()
         dens_arr = None if dens is None else _raw(dens, np.float32)
         if dens_arr is not None and dens_arr.size != M:
@@ -102,22 +106,24 @@ class Plan:
                 None if sens_arr is None else sens_arr.ctypes.data,
                 ctypes.byref(self._h)))
         else:
-            arrs = {k: (None if v is None else np.ascontiguousarray(v))
-                    for k, v in _load.items()}
-            order = arrs.get("processing_order")
+            # converted copies stay referenced until the call returns
+            def arr(key, dtype):
+                v = _load.get(key)
+                return None if v is None else np.ascontiguousarray(v, dtype)
+            traj_s = arr("traj_sorted", np.float32)
+            di = arr("data_indices", np.uint32)
+            sdc = arr("sector_data_count", np.uint32)
+            order = arr("processing_order", np.uint32)
+            ctr = arr("sector_centers", np.uint32)
+            dens_s = arr("dens_sorted", np.float32)
+            deapo = arr("deapo", np.float32)
             n_order = 0 if order is None else order.size // 2
             ptr = lambda a: None if a is None else a.ctypes.data  # noqa: E731
             C.check(L.gnufft_plan_load(
-                ctypes.byref(d), ptr(arrs["traj_sorted"].astype(np.float32)),
-                ptr(arrs["data_indices"].astype(np.uint32)),
-                ptr(arrs["sector_data_count"].astype(np.uint32)),
-                ptr(None if order is None else order.astype(np.uint32)),
-                n_order, ptr(arrs["sector_centers"].astype(np.uint32)),
-                ptr(None if arrs.get("dens_sorted") is None else
-                    arrs["dens_sorted"].astype(np.float32)),
+                ctypes.byref(d), ptr(traj_s), ptr(di), ptr(sdc), ptr(order),
+                n_order, ptr(ctr), ptr(dens_s),
                 None if sens_arr is None else sens_arr.ctypes.data,
-                ptr(arrs["deapo"].astype(np.float32)),
-                ctypes.byref(self._h)))
+                ptr(deapo), ctypes.byref(self._h)))
         self.info = self._info()
         self.grid_shape = (
             tuple(int(v) for v in self.info.grid_dims[:2][::-1])
@@ -160,6 +166,37 @@ class Plan:
         out["traj_sorted"] = out["traj_sorted"].reshape(self.dim, self.M)
         out["processing_order"] = out["processing_order"].reshape(-1, 2)
         return out
+
+    # the precomputed-operator contract of the upstream MATLAB path
+    # (gpuNUFFT.m:101 / loadPrecomputedGpuNUFFTOperator): these arrays plus
+    # the geometry rebuild the operator without re-binning
+    PLAN_ARRAYS = ("traj_sorted", "data_indices", "sector_data_count",
+                   "processing_order", "sector_centers", "dens_sorted",
+                   "deapo")
+
+    def save(self, path) -> None:
+        """Write the plan's precomputed tables and geometry to ``path``
+        (NumPy .npz); ``Plan.from_file`` rebuilds the operator from it."""
+        t = self.tables()
+        arrays = {k: t[k] for k in self.PLAN_ARRAYS if t[k] is not None}
+        np.savez(path, img_dims=np.asarray(self.img_dims, np.uint32),
+                 kernel_width=np.uint32(self.kernel_width),
+                 sector_width=np.uint32(self.sector_width),
+                 osf=np.float32(self.osf),
+                 operator_type=np.int32(self.operator_type), **arrays)
+
+    @classmethod
+    def from_file(cls, path, sens=None, device: int = 0) -> "Plan":
+        """Plan from a file written by ``save`` (tables validated)."""
+        with np.load(path) as f:
+            tables = {k: (f[k] if k in f.files else None)
+                      for k in cls.PLAN_ARRAYS}
+            dims = [int(v) for v in f["img_dims"]]
+            if dims[2] == 0:
+                dims = dims[:2]
+            return cls.load(tables, dims, int(f["kernel_width"]),
+                            int(f["sector_width"]), float(f["osf"]), sens,
+                            int(f["operator_type"]), device=device)
 
     def set_sens(self, sens) -> None:
         if sens is None:

@@ -601,3 +601,37 @@ def rel_l2(a, b) -> float:
     a = np.asarray(a, np.complex128).ravel()
     b = np.asarray(b, np.complex128).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# --------------------------------------------------------------------------
+# CG-SENSE (matlab/demo/utils/cg_sense_2d.m:40-108, multicoil form)
+# --------------------------------------------------------------------------
+def cg_sense(op: "OracleOperator", kspace: np.ndarray, maxit: int = 10,
+             alpha: float = 0.0, mask: Optional[np.ndarray] = None):
+    """The upstream demo's own CG loop with ``op`` carrying the maps:
+    rhs = A^H (y sqrt(mask)); M(x) = A^H A x + alpha x; x0 = 0; ``maxit``
+    iterations.  Vectors in complex128, operator applications in the
+    restated single-precision operator."""
+    y = np.asarray(kspace, np.complex64)
+    if mask is not None:
+        y = (y * np.sqrt(np.asarray(mask, np.float32))).astype(np.complex64)
+    rhs = op.adjoint(y).astype(np.complex128)
+
+    def apply_m(v):
+        out = op.adjoint(op.forward(v.astype(np.complex64))).astype(
+            np.complex128)
+        return out + alpha * v if alpha else out
+
+    x = np.zeros_like(rhs)
+    r = rhs.copy()
+    p = r.copy()
+    rr = np.vdot(r, r).real
+    for _ in range(maxit):
+        ap = apply_m(p)
+        a = rr / np.vdot(p, ap)
+        x = x + a * p
+        r = r - a * ap
+        rr_new = np.vdot(r, r).real
+        p = r + (rr_new / rr) * p
+        rr = rr_new
+    return x

@@ -1,0 +1,146 @@
+"""Parity against the upstream library's own GPU run on the same inputs.
+
+The upstream DEFAULT and BALANCED operators are compiled from the upstream
+sources for sm_100a (``oracle/build_ref.sh`` -> ``oracle/_ref``; texture
+operators cannot be built with CUDA 12) and driven through their host-array
+API (``performGpuNUFFTAdj`` / ``performForwardGpuNUFFT``,
+``gpuNUFFT_operator.hpp:243-345``).  Results of this library must agree
+within 1e-5 relative L2 (both accumulate in FP32; the summation order
+differs).
+
+Only isotropic 2-D geometries are run through the upstream GPU code: its
+2-D forward tests y wrap-around against the grid width
+(``atomic_gpuNUFFT_kernels.cu:1255``), which reads outside the grid for
+anisotropic 2-D grids.
+"""
+import numpy as np
+import pytest
+
+from oracle import ref as R
+from tests.helpers import cplx, gaussian_maps, kooshball_3d, radial_2d, rel_l2
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not R.available(),
+                                 reason="upstream build (oracle/_ref) absent")]
+
+TOL = 1e-5
+
+
+def _ramp(traj):
+    r = np.sqrt((traj.astype(np.float64) ** 2).sum(0))
+    return (r / r.max()).astype(np.float32)
+
+
+CASES = {
+    # name: (dims, traj factory, coils, osf, kw, sw, dens, sens)
+    "2d128_radial_ramp_1coil": ((128, 128), lambda r: radial_2d(64, 256), 1,
+                                2.0, 3, 8, "ramp", False),
+    "2d64_radial_4coil_sens": ((64, 64), lambda r: radial_2d(48, 128), 4,
+                               2.0, 3, 8, "uniform", True),
+    "2d48_uniform_kw5_osf1.5": ((48, 48),
+                                lambda r: r.uniform(-0.5, 0.5, (2, 3000)), 2,
+                                1.5, 5, 6, None, False),
+    "3d32_koosh_3coil": ((32, 32, 32), lambda r: kooshball_3d(400, 64), 3,
+                         2.0, 3, 8, "uniform", False),
+    "3d24_koosh_4coil_sens": ((24, 24, 24), lambda r: kooshball_3d(300, 48),
+                              4, 2.0, 3, 8, None, True),
+    "3d_aniso_uniform_kw4": ((24, 24, 12),
+                             lambda r: r.uniform(-0.5, 0.5, (3, 5000)), 2,
+                             1.5, 4, 5, "uniform", False),
+}
+
+
+def _inputs(name, seed):
+    dims, mk, C, osf, kw, sw, dens, sens = CASES[name]
+    rng = np.random.default_rng(seed)
+    traj = np.ascontiguousarray(mk(rng), np.float32)
+    M = traj.shape[1]
+    w = None
+    if dens == "ramp":
+        w = _ramp(traj)
+    elif dens == "uniform":
+        w = rng.uniform(0.2, 1.0, M).astype(np.float32)
+    maps = gaussian_maps(C, dims[::-1], rng) if sens else None
+    return traj, dims, C, osf, kw, sw, w, maps, rng
+
+
+@pytest.mark.parametrize("balanced", [False, True])
+@pytest.mark.parametrize("name", list(CASES))
+def test_matches_upstream_gpu_run(name, balanced):
+    import gpunufft_b200 as G
+    traj, dims, C, osf, kw, sw, w, maps, rng = _inputs(name, 11)
+    M = traj.shape[1]
+    op_type = G.BALANCED if balanced else G.DEFAULT
+    ours = G.Plan(traj, dims, kw, sw, osf, w, maps, op_type)
+    up = R.RefGpuOperator(traj, dims, C, kw, sw, osf, dens=w, sens=maps,
+                          balance=balanced)
+    up1 = None
+    try:
+        k = cplx(rng, C, M)
+        got = np.asarray(ours.adjoint(k, G.DEAPODIZATION)).ravel()
+        exp = up.adjoint(k, G.DEAPODIZATION, out_len=got.size)
+        err = rel_l2(got, exp)
+        assert err < TOL, err
+        if maps is None:
+            # The upstream host API returns intact CONVOLUTION / FFT stage
+            # output only for the first coil chunk (gpuNUFFT_operator.cpp:
+            # 737-740, 800-806): compare those stages on one coil.
+            up1 = R.RefGpuOperator(traj, dims, 1, kw, sw, osf, dens=w,
+                                   balance=balanced)
+            for stage in (G.CONVOLUTION, G.FFT):
+                got = np.asarray(ours.adjoint(k[:1], stage)).ravel()
+                exp = up1.adjoint(k[:1], stage, out_len=got.size)
+                err = rel_l2(got, exp)
+                assert err < TOL, (stage, err)
+        img_shape = tuple(dims[::-1])
+        x = cplx(rng, *img_shape) if maps is not None else \
+            cplx(rng, C, *img_shape)
+        got = np.asarray(ours.forward(x))
+        if len(dims) == 2 and C > 1 and not balanced:
+            # The upstream DEFAULT 2-D forward processes several coils per
+            # block (blockDim.z > 1), and every z-thread advances the shared
+            # sector counter (atomic_gpuNUFFT_kernels.cu:1361), so sectors
+            # are skipped.  Compare that variant one coil at a time: the
+            # maps applied to the image, a one-coil upstream operator.
+            if up1 is None:
+                up1 = R.RefGpuOperator(traj, dims, 1, kw, sw, osf, dens=w,
+                                       balance=False)
+            xs = [maps[c] * x if maps is not None else x[c]
+                  for c in range(C)]
+            exp = np.concatenate([up1.forward(v) for v in xs])
+        else:
+            exp = up.forward(x)
+        err = rel_l2(got, exp)
+        assert err < TOL, err
+    finally:
+        if up1 is not None:
+            up1.close()
+        up.close()
+        ours.close()
+
+
+def test_matches_upstream_gpu_run_3d128_32coil():
+    """The published configuration: 3D 128^3, osf 2, kw 3, sw 8, 32 coils,
+    kooshball 8192 x 256, Gaussian-profile maps; forward and coil-combined
+    adjoint against the upstream BALANCED operator."""
+    import gpunufft_b200 as G
+    rng = np.random.default_rng(3)
+    dims = (128, 128, 128)
+    C = 32
+    traj = kooshball_3d(8192, 256)
+    M = traj.shape[1]
+    maps = gaussian_maps(C, dims, rng)
+    ours = G.Plan(traj, dims, 3, 8, 2.0, None, maps, G.BALANCED)
+    up = R.RefGpuOperator(traj, dims, C, 3, 8, 2.0, sens=maps, balance=True)
+    try:
+        k = cplx(rng, C, M)
+        got = np.asarray(ours.adjoint(k)).ravel()
+        exp = up.adjoint(k, G.DEAPODIZATION, out_len=got.size)
+        assert rel_l2(got, exp) < TOL, rel_l2(got, exp)
+        x = cplx(rng, *dims)
+        got = np.asarray(ours.forward(x))
+        exp = up.forward(x)
+        assert rel_l2(got, exp) < TOL, rel_l2(got, exp)
+    finally:
+        up.close()
+        ours.close()
