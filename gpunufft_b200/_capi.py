@@ -33,6 +33,7 @@ EXPORTED = (
     "gnufft_forward_device", "gnufft_set_timing", "gnufft_get_stage_times",
     "gnufft_last_error", "gnufft_status_string", "gnufft_version",
     "gnufft_adjoint_convolution_noalloc",
+    "gnufft_traj_grad_device",
 )
 
 
@@ -119,6 +120,8 @@ def lib() -> ctypes.CDLL:
         f.argtypes = [_P, _P, _P, _U, _I, _P]
     L.gnufft_adjoint_convolution_noalloc.restype = st
     L.gnufft_adjoint_convolution_noalloc.argtypes = [_P, _P, _P, _U, _P]
+    L.gnufft_traj_grad_device.restype = st
+    L.gnufft_traj_grad_device.argtypes = [_P, _P, _P, _U, _P, _P]
     L.gnufft_set_timing.restype = st
     L.gnufft_set_timing.argtypes = [_P, ctypes.c_int]
     L.gnufft_get_stage_times.restype = st

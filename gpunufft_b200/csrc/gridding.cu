@@ -551,16 +551,21 @@ __global__ void k_zero_targets(const int *__restrict__ targets, Geo g, int C,
 // --------------------------------------------------------------------------
 // adjoint as a product with the interpolation matrix (CSR by grid cell)
 // --------------------------------------------------------------------------
-// One block per (grid row, 64-cell x chunk, coil group).  Each warp slot
-// accumulates whole cells -- all CG coils in its lanes, in registers -- from
-// the cell's (sample, weight) list, reading 8*CG contiguous bytes of the
-// sorted k-space per entry; the chunk is then written once per coil with
-// coalesced stores (INVERSE fftshift folded into the store position).  No
-// atomics, no read-modify-write, fixed summation order.
+// One block per (grid row, 64-cell x chunk, coil group).  The chunk's
+// nonzeros (a contiguous CSR range) are split into equal shares, one per
+// warp slot ("unit"); a unit streams its share with the CG coils of a
+// sample in its lanes (8*CG contiguous bytes of the sorted k-space per
+// entry) and keeps a running sum per cell in registers.  A cell inside one
+// unit's share is stored once.  A cell cut by share boundaries is summed by
+// the unit where it starts: after a barrier it adds the partial sums of the
+// following units that continue the cell, in unit order.  So the summation
+// order is fixed (results are bitwise reproducible) and there are no
+// atomics.  The chunk is then written once per coil with coalesced stores
+// (INVERSE fftshift folded into the store position).
 constexpr int kSpmmCells = 64;
 
 template <int CG>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     k_adjoint_spmm(const uint32_t *__restrict__ row_off,
                    const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
                    int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
@@ -570,6 +575,11 @@ __global__ void __launch_bounds__(kThreads)
   constexpr int B = 8;                // entries per batch
   __shared__ float2 acc_s[kSpmmCells][CG + 1];
   __shared__ uint32_t s_off[kSpmmCells + 1];
+  // partial sums of cells cut by share boundaries: head = the unit's first
+  // cell when it started in an earlier share, tail = its last cell when it
+  // started in this share and continues in the next
+  __shared__ float2 part_head[NU][CG], part_tail[NU][CG];
+  __shared__ int head_cell[NU], tail_cell[NU];
   const int x0 = blockIdx.y * kSpmmCells;
   const int row = blockIdx.x;  // y + G1 * z
   const int group = blockIdx.z;
@@ -604,6 +614,8 @@ __global__ void __launch_bounds__(kThreads)
   }
   for (int i = threadIdx.x; i < kSpmmCells * (CG + 1); i += kThreads)
     (&acc_s[0][0])[i] = make_float2(0.f, 0.f);
+  for (int i = threadIdx.x; i < NU; i += kThreads)
+    head_cell[i] = tail_cell[i] = -1;
   __syncthreads();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -657,9 +669,15 @@ __global__ void __launch_bounds__(kThreads)
           break;
         const uint32_t k = k0 + u;
         while (k >= bound)
-        {  // cell boundary: flush the running sum
-          atomicAdd(&acc_s[cell][coil].x, ax);
-          atomicAdd(&acc_s[cell][coil].y, ay);
+        {  // cell boundary: the cell is complete within this share
+          if (s_off[cell] < u0)
+          {
+            part_head[unit][coil] = make_float2(ax, ay);
+            if (coil == 0)
+              head_cell[unit] = cell;
+          }
+          else
+            acc_s[cell][coil] = make_float2(ax, ay);
           ax = ay = 0.f;
           ++cell;
           bound = s_off[cell + 1];
@@ -669,8 +687,34 @@ __global__ void __launch_bounds__(kThreads)
         ay = __fmaf_rn(w, v[u].y, ay);
       }
     }
-    atomicAdd(&acc_s[cell][coil].x, ax);
-    atomicAdd(&acc_s[cell][coil].y, ay);
+    if (s_off[cell] < u0)
+    {
+      part_head[unit][coil] = make_float2(ax, ay);
+      if (coil == 0)
+        head_cell[unit] = cell;
+    }
+    else if (bound <= u1)
+      acc_s[cell][coil] = make_float2(ax, ay);
+    else
+    {
+      part_tail[unit][coil] = make_float2(ax, ay);
+      if (coil == 0)
+        tail_cell[unit] = cell;
+    }
+  }
+  __syncthreads();
+  {  // the unit where a cut cell starts adds the continuations in order
+    const int tc = tail_cell[unit];
+    if (tc >= 0)
+    {
+      float2 sum = part_tail[unit][coil];
+      for (int v = unit + 1; v < NU && head_cell[v] == tc; ++v)
+      {
+        sum.x = __fadd_rn(sum.x, part_head[v][coil].x);
+        sum.y = __fadd_rn(sum.y, part_head[v][coil].y);
+      }
+      acc_s[tc][coil] = sum;
+    }
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)

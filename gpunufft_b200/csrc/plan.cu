@@ -30,6 +30,7 @@
 #include "geometry.hpp"
 #include "gridding.cuh"
 #include "planview.hpp"
+#include "trajgrad.cuh"
 
 using namespace gnufft;
 
@@ -79,6 +80,8 @@ struct gnufft_plan
   DeviceBuffer lut, traj_sorted, di, sec_sorted, dens_sorted, cand, cand_off;
   DeviceBuffer adj_items, split_targets, fwd_items, deapo, sens;
   DeviceBuffer w_rows, w_nz;  // interpolation matrix, CSR by grid cell
+  DeviceBuffer dlut;          // kernel derivative table (trajectory gradient)
+  float dlut_mult = 0.f;
   size_t nnz = 0;
   int n_adj_items = 0, n_split = 0, n_fwd_items = 0;
   size_t n_cand = 0;
@@ -335,7 +338,11 @@ void set_sens_host(gnufft_plan &p, const void *sens, uint32_t n_coils)
   const size_t n = (size_t)n_coils * p.g.img_count;
   const float2 *s = static_cast<const float2 *>(sens);
   p.sens_h.assign(s, s + n);
-  upload(p.sens, p.sens_h.data(), n, p.stream);
+  // keep the device buffer when it is large enough (no free / malloc, which
+  // would synchronise the device, when maps are swapped between requests)
+  p.sens.ensure(n * sizeof(float2));
+  GN_CUDA(cudaMemcpyAsync(p.sens.get(), p.sens_h.data(), n * sizeof(float2),
+                          cudaMemcpyHostToDevice, p.stream));
   p.sens_coils = n_coils;
 }
 
@@ -599,6 +606,35 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
   p.mark(3, s);
   p.mark(6, s);
   p.mark(7, s);
+}
+
+// Trajectory gradient: the forward's prepare + FFT, then the derivative
+// interpolation against the k-space weights u [C][M].
+void traj_grad(gnufft_plan &p, const float2 *img, const float2 *u, uint32_t C,
+               float *out, cudaStream_t s, const float2 *sens)
+{
+  const Geo &g = p.g;
+  if (!p.dlut.get())
+  {
+    std::vector<float> tab;
+    deriv_lut_fill(g, p.desc.osf, kDerivLutLen, tab, p.dlut_mult);
+    upload(p.dlut, tab.data(), tab.size(), s);
+  }
+  p.grid.ensure((size_t)C * g.grid_count * sizeof(float2));
+  float2 *grid = p.grid.as<float2>();
+  launch_forward_prepare(img, sens, p.deapo.as<float>(), g, (int)C, false,
+                         grid, s);
+  cufftHandle h = p.fft_plan((int)C);
+  check_cufft(cufftSetStream(h, s), "cufftSetStream");
+  check_cufft(cufftExecC2C(h, (cufftComplex *)grid, (cufftComplex *)grid,
+                           CUFFT_FORWARD),
+              "cufftExecC2C forward");
+  launch_traj_grad(p.traj_sorted.as<float>(), p.sec_sorted.as<uint32_t>(),
+                   p.di.as<uint32_t>(),
+                   p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
+                   p.lut.as<float>(), p.dlut.as<float>(), kDerivLutLen,
+                   p.dlut_mult, p.M, (int)C, g.fft_scale, u, out, s);
+  p.launches += 3;
 }
 
 size_t adjoint_out_count(const gnufft_plan &p, uint32_t C, int stage)
@@ -995,6 +1031,24 @@ gnufft_status gnufft_forward_host(gnufft_plan *p, const void *image,
                             cudaMemcpyDeviceToHost, s));
     GN_CUDA(cudaStreamSynchronize(s));
     collect_times(*p, s);
+  });
+}
+
+gnufft_status gnufft_traj_grad_device(gnufft_plan *p, const void *image,
+                                      const void *kspace_weights,
+                                      uint32_t n_coils, float *grad_traj,
+                                      void *stream)
+{
+  if (!p || !image || !kspace_weights || !grad_traj)
+    return (gnufft_status)fail(kInvalidArgument, "NULL argument");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    check_coils(*p, n_coils);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    p->launches = 0;
+    traj_grad(*p, (const float2 *)image, (const float2 *)kspace_weights,
+              n_coils, grad_traj, s, p->sens.as<float2>());
+    p->times.launches = p->launches;
   });
 }
 

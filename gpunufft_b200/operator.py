@@ -278,6 +278,28 @@ class Plan:
                                             out.ctypes.data, nc, int(output)))
         return out.reshape(nc, self.M)
 
+    def traj_grad(self, image, kspace_weights,
+                  n_coils: Optional[int] = None):
+        """grad[a][j] = sum_c Re(conj(u[c][j]) * d forward(image)[c][j] /
+        d k_a[j]) for CUDA tensors (float32 (dim, M), original order)."""
+        if not (_is_cuda_tensor(image) and _is_cuda_tensor(kspace_weights)):
+            raise TypeError("traj_grad takes CUDA tensors")
+        x = image.reshape(-1).to(torch.complex64).contiguous()
+        u = kspace_weights.reshape(-1).to(torch.complex64).contiguous()
+        nc = n_coils or u.numel() // self.M
+        if u.numel() != nc * self.M:
+            raise ValueError("k-space weights do not match the plan")
+        need = self.n_img if self.n_sens else nc * self.n_img
+        if x.numel() != need:
+            raise ValueError("image size does not match the plan")
+        out = torch.empty((self.dim, self.M), dtype=torch.float32,
+                          device=u.device)
+        stream = torch.cuda.current_stream(u.device).cuda_stream
+        C.check(C.lib().gnufft_traj_grad_device(
+            self._h, x.data_ptr(), u.data_ptr(), nc, out.data_ptr(),
+            ctypes.c_void_p(stream)))
+        return out
+
     def close(self) -> None:
         if getattr(self, "_h", None) and self._h.value:
             C.lib().gnufft_plan_destroy(self._h)

@@ -1,0 +1,303 @@
+"""Serving loop for CG-SENSE reconstruction requests with continuous
+batching and memory-based admission.
+
+A request carries a trajectory, multicoil k-space, sensitivity maps and a
+CG iteration count (the body of ``matlab/demo/utils/cg_sense_2d.m:40-108``).
+The server keeps operators resident per trajectory (sector tables,
+interpolation matrix, cuFFT plans: ``PlanCache``), admits queued requests
+whenever a slot and enough device memory are free, and advances every
+admitted request by one CG iteration per scheduler round, each request on
+its own CUDA stream.  Requests that arrive while others are on the GPU join
+at the next round; finished requests leave and free their slot and memory
+at once, so work of different sizes overlaps on the device.  Every
+iteration is stream-ordered and needs no host synchronisation; the
+scheduler only polls CUDA events.
+
+Results do not depend on the mix: a request's arithmetic runs on its own
+plan instance and stream in a fixed order.
+"""
+from __future__ import annotations
+
+import collections
+import dataclasses
+import hashlib
+import time
+from typing import Deque, Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from . import _capi as C
+from .cg_sense import _dot
+from .operator import Plan
+
+
+@dataclasses.dataclass
+class Request:
+    traj: np.ndarray                 # (dim, M) float32 in [-0.5, 0.5)
+    img_dims: Tuple[int, ...]        # (width, height[, depth])
+    kspace: np.ndarray               # (C, M) complex64
+    sens: np.ndarray                 # (C, [depth,] height, width) complex64
+    n_iter: int = 10
+    dens: Optional[np.ndarray] = None
+    alpha: float = 0.0
+    kernel_width: int = 3
+    sector_width: int = 8
+    osf: float = 2.0
+    arrival: float = 0.0             # seconds, relative to the server clock
+    rid: int = -1
+    # filled in by the server
+    result: Optional[np.ndarray] = None
+    admitted: float = 0.0
+    finished: float = 0.0
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def _key(req: Request) -> str:
+    h = hashlib.sha1()
+    h.update(np.ascontiguousarray(req.traj, np.float32).tobytes())
+    if req.dens is not None:
+        h.update(np.ascontiguousarray(req.dens, np.float32).tobytes())
+    h.update(repr((tuple(req.img_dims), req.kernel_width, req.sector_width,
+                   float(req.osf))).encode())
+    return h.hexdigest()
+
+
+def estimate_bytes(req: Request) -> int:
+    """Device bytes a request needs while it runs: the operator's tables
+    and scratch plus the CG vectors."""
+    dims = [v for v in req.img_dims if v]
+    dim = len(dims)
+    M = req.traj.shape[1]
+    Cn = req.kspace.shape[0]
+    N = int(np.prod(dims))
+    G = int(np.prod([int(np.ceil(v * req.osf)) for v in dims]))
+    lanes = Cn if Cn <= 16 else (Cn + 31) // 32 * 32
+    kw = req.kernel_width
+    nnz = M * kw ** dim
+    tables = M * (4 * dim + 16) + 8 * nnz + 4 * G + 4 * N
+    scratch = 8 * M * lanes + 2 * 8 * Cn * G          # sorted k-space, grid,
+    scratch += 8 * Cn * G                              # cuFFT work area
+    vectors = 8 * Cn * M * 2 + 8 * Cn * N + 8 * N * 6  # data, maps, CG
+    return int(tables + scratch + vectors)
+
+
+class PlanCache:
+    """Operators resident per trajectory.  Several instances of one
+    trajectory's operator exist only while several requests use it at the
+    same time; idle instances stay cached until memory is needed."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        self.free: Dict[str, List[Plan]] = collections.defaultdict(list)
+        self.busy: Dict[int, str] = {}
+        self.lru: "collections.OrderedDict[str, float]" = \
+            collections.OrderedDict()
+        self.hits = 0
+        self.misses = 0
+
+    def acquire(self, req: Request) -> Plan:
+        key = _key(req)
+        self.lru[key] = time.perf_counter()
+        self.lru.move_to_end(key)
+        if self.free[key]:
+            self.hits += 1
+            p = self.free[key].pop()
+        else:
+            self.misses += 1
+            p = Plan(req.traj, req.img_dims, req.kernel_width,
+                     req.sector_width, req.osf, req.dens, None, C.BALANCED,
+                     device=self.device)
+        self.busy[id(p)] = key
+        return p
+
+    def release(self, p: Plan) -> None:
+        key = self.busy.pop(id(p))
+        self.free[key].append(p)
+
+    def idle_bytes(self) -> int:
+        return sum(p.info.device_bytes for ps in self.free.values()
+                   for p in ps)
+
+    def evict_one(self) -> bool:
+        """Drop one idle instance, least recently used trajectory first."""
+        for key in list(self.lru):
+            if self.free.get(key):
+                self.free[key].pop().close()
+                if not self.free[key] and key not in self.busy.values():
+                    del self.lru[key]
+                return True
+        return False
+
+    def clear(self) -> None:
+        for ps in self.free.values():
+            for p in ps:
+                p.close()
+        self.free.clear()
+
+
+class _Active:
+    """A request on the GPU: its plan instance, stream and CG state."""
+
+    def __init__(self, req: Request, plan: Plan, device: int):
+        self.req = req
+        self.plan = plan
+        self.stream = torch.cuda.Stream(device=device)
+        self.done_event = torch.cuda.Event()
+        self.it = 0
+        with torch.cuda.stream(self.stream):
+            dev = torch.device("cuda", device)
+            self.y = torch.from_numpy(np.ascontiguousarray(
+                req.kspace, np.complex64)).to(dev, non_blocking=True)
+            plan.set_sens(req.sens)
+            rhs = plan.adjoint(self.y)
+            self.x = torch.zeros_like(rhs)
+            self.r = rhs
+            self.p = rhs.clone()
+            self.rr = _dot(self.r, self.r).real
+
+    def step(self) -> None:
+        """Enqueue one CG iteration on this request's stream."""
+        with torch.cuda.stream(self.stream):
+            ap = self.plan.adjoint(self.plan.forward(self.p))
+            if self.req.alpha:
+                ap = ap + self.req.alpha * self.p
+            a = self.rr / _dot(self.p, ap)
+            self.x = self.x + a * self.p
+            self.r = self.r - a * ap
+            rr_new = _dot(self.r, self.r).real
+            self.p = self.r + (rr_new / self.rr) * self.p
+            self.rr = rr_new
+            self.it += 1
+            if self.it == self.req.n_iter:
+                self.out = torch.empty(self.x.shape, dtype=self.x.dtype,
+                                       pin_memory=True)
+                self.out.copy_(self.x, non_blocking=True)
+                self.done_event.record(self.stream)
+
+    def finished(self) -> bool:
+        return self.it == self.req.n_iter and self.done_event.query()
+
+
+class Server:
+    """Continuous-batching CG-SENSE server on one GPU.
+
+    max_slots: requests on the GPU at once; memory_budget: device bytes the
+    server may hold for running requests and cached operators (default:
+    90 % of the free memory at start)."""
+
+    def __init__(self, device: int = 0, max_slots: int = 8,
+                 memory_budget: Optional[int] = None):
+        self.device = device
+        torch.cuda.set_device(device)
+        free, _ = torch.cuda.mem_get_info(device)
+        self.budget = int(memory_budget if memory_budget is not None
+                          else 0.9 * free)
+        self.max_slots = max_slots
+        self.cache = PlanCache(device)
+        self.queue: Deque[Request] = collections.deque()
+        self.active: List[_Active] = []
+        self.done: List[Request] = []
+        self.in_use = 0
+        self.peak_in_use = 0
+        self.peak_device_used = 0
+        self.max_concurrent = 0
+        self._t0 = time.perf_counter()
+        self._free0 = free
+
+    def now(self) -> float:
+        return time.perf_counter() - self._t0
+
+    def submit(self, req: Request) -> None:
+        if estimate_bytes(req) > self.budget:
+            raise ValueError("request larger than the server's memory budget")
+        if req.arrival <= 0:
+            req.arrival = self.now()
+        self.queue.append(req)
+
+    def _admit(self) -> None:
+        while self.queue and len(self.active) < self.max_slots:
+            req = self.queue[0]
+            need = estimate_bytes(req)
+            while (self.in_use + need + self.cache.idle_bytes() > self.budget
+                   and self.cache.evict_one()):
+                pass
+            if self.in_use + need > self.budget:
+                break                       # wait for memory to free up
+            self.queue.popleft()
+            req.admitted = self.now()
+            plan = self.cache.acquire(req)
+            self.active.append(_Active(req, plan, self.device))
+            self.in_use += need
+            self.peak_in_use = max(self.peak_in_use, self.in_use)
+        self.max_concurrent = max(self.max_concurrent, len(self.active))
+
+    def _retire(self) -> None:
+        keep = []
+        for a in self.active:
+            if a.finished():
+                a.req.result = a.out.numpy().copy()
+                a.req.finished = self.now()
+                self.cache.release(a.plan)
+                self.in_use -= estimate_bytes(a.req)
+                self.done.append(a.req)
+            else:
+                keep.append(a)
+        self.active = keep
+
+    def round(self) -> None:
+        """One scheduler round: retire, admit, one iteration per request."""
+        self._retire()
+        self._admit()
+        for a in self.active:
+            if a.it < a.req.n_iter:
+                a.step()
+        free, total = torch.cuda.mem_get_info(self.device)
+        self.peak_device_used = max(self.peak_device_used, total - free)
+
+    def run(self, arrivals: Sequence[Request], timeout: float = 600.0):
+        """Replay ``arrivals`` (sorted by ``arrival`` seconds from now) and
+        serve until all are done.  Returns the finished requests."""
+        pending = collections.deque(sorted(arrivals, key=lambda r: r.arrival))
+        self._t0 = time.perf_counter()
+        n = len(pending)
+        while len(self.done) < n:
+            t = self.now()
+            if t > timeout:
+                raise TimeoutError("serving did not finish")
+            while pending and pending[0].arrival <= t:
+                self.queue.append(pending.popleft())
+            if not self.active and not self.queue and pending:
+                time.sleep(min(0.001, max(0.0, pending[0].arrival - t)))
+                continue
+            self.round()
+            if self.active and all(a.it == a.req.n_iter for a in self.active):
+                time.sleep(0.0002)      # everything enqueued: wait a little
+        torch.cuda.synchronize(self.device)
+        return list(self.done)
+
+    def stats(self) -> dict:
+        lat = np.array([r.latency for r in self.done]) * 1e3
+        span = (max(r.finished for r in self.done) -
+                min(r.arrival for r in self.done)) if self.done else 0.0
+        return {
+            "requests": len(self.done),
+            "p50_ms": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_ms": float(np.percentile(lat, 99)) if len(lat) else None,
+            "throughput_rps": len(self.done) / span if span > 0 else None,
+            "max_concurrent": self.max_concurrent,
+            "peak_hbm_gb": self.peak_device_used / 1e9,
+            "peak_admitted_estimate_gb": self.peak_in_use / 1e9,
+            "plan_cache_hits": self.cache.hits,
+            "plan_cache_misses": self.cache.misses,
+        }
+
+    def close(self) -> None:
+        torch.cuda.synchronize(self.device)
+        for a in self.active:
+            self.cache.release(a.plan)
+        self.active = []
+        self.cache.clear()

@@ -222,6 +222,20 @@ GNUFFT_API gnufft_status gnufft_adjoint_convolution_noalloc(
     gnufft_plan *plan, const void *kspace, void *grid, uint32_t n_coils,
     void *stream);
 
+/* Gradient of a real loss with respect to the trajectory (no upstream
+ * counterpart; used by the differentiable operator).  With y = forward(image)
+ * (the plan's maps and density weights included) and kspace_weights u
+ * [n_coils][M] (original order, device), writes
+ *   grad_traj[a][j] = sum_c Re( conj(u[c][j]) * d y[c][j] / d k_a[j] )
+ * (float32 [dim][M], device), the derivative taken through the Kaiser-Bessel
+ * interpolation of the oversampled spectrum.  For the adjoint x = A^H y and
+ * dL/dx = v, pass image = v and kspace_weights = y.  image as for
+ * gnufft_forward_device.  Ordered on `stream`. */
+GNUFFT_API gnufft_status gnufft_traj_grad_device(gnufft_plan *plan, const void *image,
+                                      const void *kspace_weights,
+                                      uint32_t n_coils, float *grad_traj,
+                                      void *stream);
+
 /* Device time (ms) of the stages of the last call on this plan, measured
  * with CUDA events when timing is enabled (gnufft_set_timing). */
 typedef struct gnufft_stage_times {
