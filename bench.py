@@ -451,6 +451,10 @@ def run_gpu_arm(args, rank, world, dist):
     if args.ref_gpu_steps > 0:
         ref_gpu = reference_gpu(inp, args.ref_gpu_steps)
 
+    served = None
+    if args.serve_requests > 0:
+        served = serving_run(dev, args.serve_requests, seed=rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -500,6 +504,7 @@ def run_gpu_arm(args, rank, world, dist):
                       "batched_over_plain": (value / plain_value
                                              if plain_value else None)},
             "reference_gpu": ref_gpu,
+            "served": served,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -510,15 +515,176 @@ def run_gpu_arm(args, rank, world, dist):
     plan.close()
 
 
+def serving_run(dev, n_requests, seed=0):
+    """Poisson arrivals (mean 50 requests/s) of mixed CG-SENSE requests, 10
+    iterations each: 2-D radial/spiral 128-384^2 with 1-32 coils and
+    20k-400k samples, or (one in eight) 3-D kooshball 96^3-128^3 with 8-16
+    coils and 0.5M-1M samples.  Trajectories come from a pool of ten (so
+    operators are reused); maps per (size, coils).  Returns the server's
+    statistics."""
+    from gpunufft_b200.batch import spiral_trajectory
+    from gpunufft_b200.serving import Request, Server
+    rng = np.random.default_rng(seed)
+    pool = []
+    for i in range(10):
+        if i < 8:
+            size = int(rng.choice([128, 192, 256, 384]))
+            M = int(rng.integers(20_000, 400_001))
+            if i % 2:
+                traj = radial2d(max(1, M // (2 * size)), 2 * size)
+            else:
+                traj = spiral_trajectory(int(rng.integers(8, 49)), M, rng)
+            pool.append(((size, size), traj))
+        else:
+            size = int(rng.choice([96, 128]))
+            M = int(rng.integers(500_000, 1_000_001))
+            nr = 2 * size
+            pool.append(((size,) * 3, kooshball(max(1, M // nr), nr)))
+    maps_cache = {}
+
+    def maps_for(dims, C):
+        key = (dims, C)
+        if key not in maps_cache:
+            shape = dims[::-1]
+            grids = np.meshgrid(*[np.linspace(-0.5, 0.5, n, dtype=np.float32)
+                                  for n in shape], indexing="ij")
+            m = np.empty((C,) + shape, np.complex64)
+            rss = np.zeros(shape, np.float32)
+            for c in range(C):
+                v = rng.standard_normal(len(shape))
+                cen = 0.6 * v / np.linalg.norm(v)
+                r2 = sum((g - cc) ** 2 for g, cc in zip(grids, cen))
+                m[c] = np.exp(-r2 / 0.3)
+                rss += np.abs(m[c]) ** 2
+            m /= np.sqrt(rss)
+            maps_cache[key] = m
+        return maps_cache[key]
+
+    reqs = []
+    t = 0.0
+    for i in range(n_requests):
+        t += rng.exponential(1 / 50.0)
+        dims, traj = pool[int(rng.integers(0, 10))]
+        C = (int(rng.integers(8, 17)) if len(dims) == 3 else
+             int(rng.integers(1, 33)))
+        M = traj.shape[1]
+        k = (rng.standard_normal((C, M), dtype=np.float32) + 1j *
+             rng.standard_normal((C, M), dtype=np.float32)).astype(
+                 np.complex64)
+        reqs.append(Request(traj=traj, img_dims=dims, kspace=k,
+                            sens=maps_for(dims, C), n_iter=10, arrival=t,
+                            rid=i))
+    srv = Server(device=dev, max_slots=8)
+    try:
+        srv.run(reqs)
+        st = srv.stats()
+    finally:
+        srv.close()
+    st["workload"] = (f"{n_requests} CG-SENSE requests x 10 iterations, "
+                      f"Poisson 50/s, 2-D 128-384^2 / 3-D 96-128^3 mix")
+    return st
+
+
+def run_batch_arm(args, rank, world):
+    """64 uneven 2-D spiral operators (image 96-320^2, 8-32 coils, 10k-120k
+    samples, osf 1.25-2, kernel width 3-5; sector width and forward tile
+    from the autotuner): fwd + adj of every instance per step, replayed
+    from one CUDA graph, against the plain per-instance loop."""
+    import torch
+
+    import gpunufft_b200 as G
+    from gpunufft_b200.batch import BatchedOperator, autotune, \
+        spiral_instances
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    specs = spiral_instances(64, seed=rank)
+    rng = np.random.default_rng(rank)
+    plans, coils, tuned = [], [], []
+    t0 = time.perf_counter()
+    for s in specs:
+        shape = s["img_dims"][::-1]
+        grids = np.meshgrid(*[np.linspace(-0.5, 0.5, n) for n in shape],
+                            indexing="ij")
+        maps = []
+        for c in range(s["n_coils"]):
+            a = 2 * math.pi * c / s["n_coils"]
+            cen = (0.6 * math.sin(a), 0.6 * math.cos(a))
+            r2 = sum((g - cc) ** 2 for g, cc in zip(grids, cen))
+            ramp = sum(rng.uniform(-2, 2) * g for g in grids)
+            maps.append(np.exp(-r2 / 0.3) * np.exp(1j * ramp))
+        maps = np.array(maps)
+        maps = (maps / np.sqrt((np.abs(maps) ** 2).sum(0))).astype(
+            np.complex64)
+        tr = autotune(s["traj"], s["img_dims"], s["n_coils"],
+                      s["kernel_width"], s["osf"], sens=maps, reps=2,
+                      sector_widths=(6, 8, 12), tile_coils=(0, 8, 16),
+                      device=dev)
+        tuned.append((tr.sector_width, tr.tile_coils))
+        plans.append(G.Plan(s["traj"], s["img_dims"], s["kernel_width"],
+                            tr.sector_width, s["osf"], None, maps, G.BALANCED,
+                            device=dev, tile_coils=tr.tile_coils))
+        coils.append(s["n_coils"])
+    tune_s = time.perf_counter() - t0
+    bo = BatchedOperator(plans, coils, n_streams=8, device=dev)
+    for x in bo.img_in:
+        x.copy_(torch.randn_like(x))
+    for k in bo.k_in:
+        k.copy_(torch.randn_like(k))
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps
+
+    ms_graph = timed(lambda: (bo.replay("forward"), bo.replay("adjoint")))
+    ms_plain = timed(lambda: (bo.plain("forward"), bo.plain("adjoint")))
+    n = len(plans)
+    if rank == 0:
+        sw_hist = {}
+        for sw, tc in tuned:
+            sw_hist[f"sw{sw}/tile{tc or 'auto'}"] = \
+                sw_hist.get(f"sw{sw}/tile{tc or 'auto'}", 0) + 1
+        print(json.dumps({
+            "metric": "uneven batch: instance fwd+adj/s, one CUDA graph vs "
+                      "plain per-instance loop",
+            "value": world * n / (ms_graph * 1e-3), "unit": "instances/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_graph, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "64 variable-density 2-D spirals, image "
+                                   "96-320^2, 8-32 coils, 10k-120k samples, "
+                                   "osf 1.25-2, kw 3-5, coil maps",
+                       "instances": n},
+            "plain": {"value": world * n / (ms_plain * 1e-3),
+                      "ms_per_step": ms_plain,
+                      "graph_over_plain": ms_plain / ms_graph},
+            "autotune": {"seconds": tune_s, "choices": sw_hist},
+        }), flush=True)
+    for p in plans:
+        p.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="3d128x32", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="3d128x32",
+                    choices=list(WORKLOADS) + ["spirals64"])
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=40,
+                    help="requests of the serving run (0: skip)")
     ap.add_argument("--ref-gpu-steps", type=int, default=2,
                     help="steps of the upstream GPU operator (0: skip)")
     args = ap.parse_args()
@@ -528,6 +694,9 @@ def main():
     dist = None
     if args.impl == "reference":
         run_reference_arm(args, rank)
+        return
+    if args.workload == "spirals64":
+        run_batch_arm(args, rank, world)
         return
     if world > 1:
         import datetime

@@ -25,6 +25,15 @@ CONVOLUTION, FFT, DEAPODIZATION, DENSITY_ESTIMATION = 0, 1, 2, 3
 FLAG_REFERENCE_ORDER = 0x1
 FLAG_PLAIN = 0x2
 
+
+def fwd_tile_flag(coils: int) -> int:
+    """GNUFFT_FLAG_FWD_TILE_COILS(coils); 0 selects automatically."""
+    if not coils:
+        return 0
+    if coils not in (1, 2, 4, 8, 16, 32):
+        raise ValueError("tile coils must be 1, 2, 4, 8, 16 or 32")
+    return (coils.bit_length()) << 8
+
 # Every entry point declared in include/gpunufft_b200.h.
 EXPORTED = (
     "gnufft_plan_create", "gnufft_plan_load", "gnufft_plan_destroy",

@@ -1360,11 +1360,17 @@ void launch_forward_interp(const FwdItem *items, int n_items,
                            const float *dens_sorted, const float2 *grid,
                            const Geo &g, const float *lut, uint32_t M, int C,
                            bool shift, float scale, float2 *out,
-                           cudaStream_t s)
+                           cudaStream_t s, int tile_coils)
 {
   if (n_items <= 0)
     return;
-  const int cg = forward_coil_group(C, g.dim, g.pad);
+  int cg = forward_coil_group(C, g.dim, g.pad);
+  if (tile_coils > 0)
+  {  // tuned tile shape, reduced until it fits in shared memory
+    cg = tile_coils > 32 ? 32 : tile_coils;
+    while (cg > 1 && forward_smem_bytes(g, cg) > 200 * 1024)
+      cg >>= 1;
+  }
 #define GN_FWD(D, CGV)                                                         \
   if (slots_for(g) == 4)                                                       \
     fwd_dispatch<D, CGV, 4>(items, n_items, traj_sorted, idx, dens_sorted,    \

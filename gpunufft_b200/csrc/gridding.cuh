@@ -96,6 +96,6 @@ void launch_forward_interp(const FwdItem *items, int n_items,
                            const float *dens_sorted, const float2 *grid,
                            const Geo &g, const float *lut, uint32_t M, int C,
                            bool shift, float scale, float2 *out,
-                           cudaStream_t s);
+                           cudaStream_t s, int tile_coils = 0);
 
 }  // namespace gnufft

@@ -70,6 +70,7 @@ struct gnufft_plan
   cudaStream_t stream = nullptr;
   bool texture = false;
   bool plain = false;
+  int fwd_tile_coils = 0;  // 0: automatic
 
   // host copies of the exported tables
   std::vector<float> lut_h, traj_sorted_h, dens_sorted_h, deapo_h;
@@ -308,6 +309,12 @@ void init_common(gnufft_plan &p, const gnufft_desc *d)
   p.texture = d->operator_type == GNUFFT_TEXTURE ||
               d->operator_type == GNUFFT_BALANCED_TEXTURE;
   p.plain = (d->flags & GNUFFT_FLAG_PLAIN) != 0;
+  {
+    const uint32_t code = (d->flags & GNUFFT_FLAG_FWD_TILE_MASK) >> 8;
+    if (code > 6)
+      throw Error(kInvalidArgument, "forward tile coil count out of range");
+    p.fwd_tile_coils = code ? 1 << (code - 1) : 0;
+  }
   std::string err;
   if (!make_geo(d->img_dims, d->osf, d->kernel_width, d->sector_width,
                 p.texture, p.g, err))
@@ -601,7 +608,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
       p.di.as<uint32_t>(),
       (p.has_dens && !dens_est) ? p.dens_sorted.as<float>() : nullptr, grid, g,
       p.lut.as<float>(), p.M, (int)C, !dens_est,
-      dens_est ? 1.0f : g.fft_scale, k, s);
+      dens_est ? 1.0f : g.fft_scale, k, s, p.fwd_tile_coils);
   p.launches += 1;
   p.mark(3, s);
   p.mark(6, s);

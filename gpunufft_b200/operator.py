@@ -52,7 +52,8 @@ class Plan:
                  sector_width: int = 8, osf: float = 2.0, dens=None,
                  sens=None, operator_type: int = C.BALANCED,
                  reference_order: bool = False, plain: bool = False,
-                 device: int = 0, _load: Optional[dict] = None):
+                 device: int = 0, tile_coils: int = 0,
+                 _load: Optional[dict] = None):
         self._h = ctypes.c_void_p()
         dims = [int(v) for v in img_dims]
         if len(dims) == 2:
@@ -86,7 +87,8 @@ class Plan:
         d.osf = float(osf)
         d.operator_type = int(operator_type)
         d.flags = ((C.FLAG_REFERENCE_ORDER if reference_order else 0) |
-                   (C.FLAG_PLAIN if plain else 0))
+                   (C.FLAG_PLAIN if plain else 0) |
+                   C.fwd_tile_flag(tile_coils))
         d.device = int(device)
         self.device = int(device)
         self.n_sens = n_sens
@@ -94,6 +96,7 @@ class Plan:
         self.sector_width = int(sector_width)
         self.osf = float(osf)
         self.operator_type = int(operator_type)
+        self.tile_coils = int(tile_coils)
         L = C.lib()
         dens_arr = None if dens is None else _raw(dens, np.float32)
         if dens_arr is not None and dens_arr.size != M:

@@ -98,6 +98,14 @@ typedef enum gnufft_output {
  * coil.  For comparisons only; the default executes all coils of a call in
  * one pass with resident maps. */
 #define GNUFFT_FLAG_PLAIN 0x2u
+/* Forward-interpolation tile shape (the autotuner's knob): coils staged per
+ * sector tile, n = 1, 2, 4, 8, 16 or 32, stored in bits 8-11 as
+ * log2(n) + 1; 0 selects automatically.  n is reduced until the tile fits
+ * in shared memory. */
+#define GNUFFT_FLAG_FWD_TILE_COILS(n)                                        \
+  ((uint32_t)((n) <= 1 ? 1 : (n) <= 2 ? 2 : (n) <= 4 ? 3 : (n) <= 8 ? 4 :   \
+              (n) <= 16 ? 5 : 6) << 8)
+#define GNUFFT_FLAG_FWD_TILE_MASK 0xF00u
 
 typedef struct gnufft_desc {
   uint32_t img_dims[3];  /* width, height, depth; depth == 0 selects 2-D */
