@@ -43,6 +43,7 @@ WORKLOADS = {
     # smaller 3D cases of the same kernels, for profiler captures
     "3d96x32": ((96, 96, 96), 32, 4608, 192, 2.0, 3, 8),
     "3d64x8": ((64, 64, 64), 8, 2048, 128, 2.0, 3, 8),
+    "3d64x32": ((64, 64, 64), 32, 2048, 128, 2.0, 3, 8),
     # 2D single-coil case (upstream CPU-runnable configuration)
     "2d128x1": ((128, 128), 1, 64, 256, 2.0, 3, 8),
 }

@@ -24,6 +24,7 @@ DEFAULT, TEXTURE, BALANCED, BALANCED_TEXTURE = 0, 1, 2, 3
 CONVOLUTION, FFT, DEAPODIZATION, DENSITY_ESTIMATION = 0, 1, 2, 3
 FLAG_REFERENCE_ORDER = 0x1
 FLAG_PLAIN = 0x2
+FLAG_CUFFT = 0x4
 
 
 def fwd_tile_flag(coils: int) -> int:

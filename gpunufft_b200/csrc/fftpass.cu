@@ -1,0 +1,662 @@
+// Separable, pruned Cartesian transforms fused with the image-space stages
+// (see fftpass.cuh).  Index maps per axis (G grid, N image, crop c = the
+// upstream crop offset, s = floor(G/2) the INVERSE fftshift):
+//   forward  FFT input n holds image pixel (n + s - c) mod G when < N
+//   adjoint  FFT output k holds image pixel (k - c - s) mod G when < N
+// (the upstream pad -> fftshift and fftshift -> crop,
+// gpuNUFFT_operator.cpp:1178-1215 and 775-806).
+#include "fftpass.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+
+#include "devutil.hpp"
+
+namespace gnufft
+{
+namespace
+{
+constexpr int kFftThreads = 256;
+
+template <int L> struct Split;
+template <> struct Split<16> { static constexpr int R1 = 4, R2 = 4; };
+template <> struct Split<32> { static constexpr int R1 = 8, R2 = 4; };
+template <> struct Split<64> { static constexpr int R1 = 8, R2 = 8; };
+template <> struct Split<128> { static constexpr int R1 = 16, R2 = 8; };
+template <> struct Split<256> { static constexpr int R1 = 16, R2 = 16; };
+template <> struct Split<512> { static constexpr int R1 = 32, R2 = 16; };
+template <> struct Split<1024> { static constexpr int R1 = 32, R2 = 32; };
+
+template <int L> struct Shape
+{
+  static constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
+  static constexpr int T = R1 > R2 ? R1 : R2;  // threads per line
+  static constexpr int NL = kFftThreads / T;   // lines per block (rows)
+  static constexpr int YP = R2 + 1;            // padded exchange row
+  static size_t smem() { return (size_t)(L + NL * R1 * YP) * sizeof(float2); }
+  // column passes: TC adjacent columns per block, so that every warp moves
+  // 32 * 8 bytes (L <= 256) of one row per access
+  static constexpr int TC = L <= 256 ? 32 : (L == 512 ? 16 : 8);
+  static constexpr int CT = TC * T;            // threads per column block
+  static size_t col_smem()
+  {
+    return (size_t)(L + TC * R1 * YP) * sizeof(float2);
+  }
+};
+
+__host__ __device__ constexpr int bitrev(int i, int R)
+{
+  int r = 0;
+  for (int b = 1; b < R; b <<= 1)
+  {
+    r = (r << 1) | (i & 1);
+    i >>= 1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ float2 cmul(float2 a, float2 b)
+{
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+__host__ __device__ constexpr int ilog2(int v)
+{
+  int r = 0;
+  while ((1 << r) < v)
+    ++r;
+  return r;
+}
+
+// In-register radix-2 DIT DFT of R points, natural order in and out.
+// w[k] = exp(-2 pi i k / RM), k < RM / 2, RM >= R (conjugated for the
+// inverse).  Every loop has a constant trip count and every index is a
+// constant, so data and roots stay in registers.
+template <int R, int RM, bool INV>
+__device__ __forceinline__ void reg_fft(float2 (&a)[R],
+                                        const float2 (&w)[RM / 2])
+{
+#pragma unroll
+  for (int i = 0; i < R; ++i)
+  {
+    const int j = bitrev(i, R);
+    if (j > i)
+    {
+      const float2 t = a[i];
+      a[i] = a[j];
+      a[j] = t;
+    }
+  }
+  constexpr int LOG = ilog2(R);
+#pragma unroll
+  for (int st = 0; st < LOG; ++st)
+  {
+    const int half = 1 << st;
+#pragma unroll
+    for (int b = 0; b < R / 2; ++b)
+    {
+      const int k = b & (half - 1);
+      const int i0 = ((b >> st) << (st + 1)) + k;
+      const int i1 = i0 + half;
+      const float2 u = a[i0];
+      float2 v = a[i1];
+      if (k != 0)
+      {
+        float2 r = w[k * (RM >> (st + 1))];
+        if (INV)
+          r.y = -r.y;
+        v = cmul(v, r);
+      }
+      a[i0] = make_float2(u.x + v.x, u.y + v.y);
+      a[i1] = make_float2(u.x - v.x, u.y - v.y);
+    }
+  }
+}
+
+// Stage 1 of a line (thread lt < R2 holds a[j] = x[lt + R2 j]): R1-point
+// DFT, twiddle, store to the line's exchange slots Y[(k1 * YP + lt) * YS]
+// (YS: stride between consecutive slots of one line, so that lines can be
+// interleaved for conflict-free access).
+template <int L> struct Rm
+{
+  static constexpr int V = Shape<L>::T;  // roots kept for the larger DFT
+};
+
+template <int L, bool INV, int YS>
+__device__ __forceinline__ void stage1(float2 (&a)[Shape<L>::R1], int lt,
+                                       const float2 (&w)[Rm<L>::V / 2],
+                                       const float2 *__restrict__ tw,
+                                       float2 *__restrict__ Y)
+{
+  using S = Shape<L>;
+  reg_fft<S::R1, Rm<L>::V, INV>(a, w);
+#pragma unroll
+  for (int k1 = 0; k1 < S::R1; ++k1)
+  {
+    float2 v = a[k1];
+    if (k1 != 0)
+    {
+      float2 r = tw[(lt * k1) & (L - 1)];
+      if (INV)
+        r.y = -r.y;
+      v = cmul(v, r);
+    }
+    Y[(k1 * S::YP + lt) * YS] = v;
+  }
+}
+
+// Stage 2 (thread lt < R1): b[k2] = X[lt + R1 k2].
+template <int L, bool INV, int YS>
+__device__ __forceinline__ void stage2(float2 (&b)[Shape<L>::R2], int lt,
+                                       const float2 (&w)[Rm<L>::V / 2],
+                                       const float2 *__restrict__ Y)
+{
+  using S = Shape<L>;
+#pragma unroll
+  for (int t = 0; t < S::R2; ++t)
+    b[t] = Y[(lt * S::YP + t) * YS];
+  reg_fft<S::R2, Rm<L>::V, INV>(b, w);
+}
+
+template <int L>
+__device__ __forceinline__ void load_reg_roots(float2 (&w)[Rm<L>::V / 2],
+                                               const float2 *tw)
+{
+  constexpr int RM = Rm<L>::V;
+#pragma unroll
+  for (int k = 0; k < RM / 2; ++k)
+    w[k] = tw[k * (L / RM)];
+}
+
+__device__ __forceinline__ void load_roots(float2 *tw, const float2 *roots,
+                                           int L)
+{
+  for (int i = threadIdx.x; i < L; i += blockDim.x)
+    tw[i] = __ldg(roots + i);
+}
+
+// --------------------------------------------------------------------------
+// column passes: lines along a strided axis, columns contiguous
+// --------------------------------------------------------------------------
+// src: planes of src_rows x ncols, dst: planes of dst_rows x ncols.  FFT
+// input n reads source row (n + in_add) mod L when < in_count (else zero);
+// FFT output k goes to row (k + out_add) mod L when < out_count.
+template <int L, bool INV>
+__global__ void __launch_bounds__(Shape<L>::CT)
+    k_fft_cols(const float2 *__restrict__ src, float2 *__restrict__ dst,
+               long long ncols, int src_rows, int dst_rows, int in_add,
+               int in_count, int out_add, int out_count,
+               const float2 *__restrict__ roots)
+{
+  using S = Shape<L>;
+  extern __shared__ float2 sm[];
+  float2 *tw = sm;
+  float2 *Ybase = sm + L;
+  load_roots(tw, roots, L);
+  const int cl = threadIdx.x % S::TC, lt = threadIdx.x / S::TC;
+  const long long col = (long long)blockIdx.x * S::TC + cl;
+  const long long plane = blockIdx.y;
+  const bool on = col < ncols;
+  // exchange slots of the block's columns interleaved: slot * TC + column
+  float2 *Y = Ybase + cl;
+  const float2 *sp = src + plane * src_rows * ncols + col;
+  float2 *dp = dst + plane * dst_rows * ncols + col;
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  if (lt < S::R2)
+  {
+    float2 a[S::R1];
+#pragma unroll
+    for (int j = 0; j < S::R1; ++j)
+    {
+      const int r = (lt + S::R2 * j + in_add) & (L - 1);
+      a[j] = (on && r < in_count) ? __ldg(sp + (long long)r * ncols)
+                                  : make_float2(0.f, 0.f);
+    }
+    stage1<L, INV, S::TC>(a, lt, w, tw, Y);
+  }
+  __syncthreads();
+  if (lt < S::R1)
+  {
+    float2 b[S::R2];
+    stage2<L, INV, S::TC>(b, lt, w, Y);
+    if (on)
+    {
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int r = (lt + S::R1 * k2 + out_add) & (L - 1);
+        if (r < out_count)
+          dp[(long long)r * ncols] = b[k2];
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
+// forward rows: sens multiply, deapodization, pad + shift, DFT along x
+// --------------------------------------------------------------------------
+// One line per (image row, coil), coil fastest: a block's lines share image
+// rows, so the image is read once per block.  Output A[c][row][k],
+// rows = N_y * N_z.
+template <int L, bool SENS>
+__global__ void __launch_bounds__(kFftThreads, L <= 256 ? 3 : 1)
+    k_fft_rows_fwd(const float2 *__restrict__ image,
+                   const float2 *__restrict__ sens,
+                   const float *__restrict__ deapo, int Nx, long long rows,
+                   long long N, int C, int in_add,
+                   const float2 *__restrict__ roots, float2 *__restrict__ A)
+{
+  using S = Shape<L>;
+  extern __shared__ float2 sm[];
+  float2 *tw = sm;
+  load_roots(tw, roots, L);
+  const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
+  const long long ln = (long long)blockIdx.x * S::NL + line;
+  const bool on = ln < rows * C;
+  const long long row = on ? ln / C : 0;
+  const int c = on ? (int)(ln - row * C) : 0;
+  float2 *Y = sm + L + line * S::R1 * S::YP;
+  const long long rbase = row * Nx;
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  if (lt < S::R2)
+  {
+    // FFT input n = lt + R2 j holds image x (n + in_add) mod L when < Nx
+    float2 a[S::R1];
+#pragma unroll
+    for (int j = 0; j < S::R1; ++j)
+    {
+      const int xp = (lt + S::R2 * j + in_add) & (L - 1);
+      float2 v = make_float2(0.f, 0.f);
+      if (on && xp < Nx)
+      {
+        const long long px = rbase + xp;
+        if (SENS)
+        {  // sensMulKernel, then deapodization (std_gpuNUFFT_kernels.cu)
+          const float2 x = __ldg(image + px);
+          const float2 s = __ldg(sens + c * N + px);
+          v.x = x.x * s.x - x.y * s.y;
+          v.y = x.x * s.y + x.y * s.x;
+        }
+        else
+          v = __ldg(image + c * N + px);
+        const float d = __ldg(deapo + px);
+        v.x = __fmul_rn(v.x, d);
+        v.y = __fmul_rn(v.y, d);
+      }
+      a[j] = v;
+    }
+    stage1<L, false, 1>(a, lt, w, tw, Y);
+  }
+  __syncthreads();
+  if (lt < S::R1 && on)
+  {
+    float2 b[S::R2];
+    stage2<L, false, 1>(b, lt, w, Y);
+    float2 *out = A + ((long long)c * rows + row) * L;
+#pragma unroll
+    for (int k2 = 0; k2 < S::R2; ++k2)
+      out[lt + S::R1 * k2] = b[k2];
+  }
+}
+
+// --------------------------------------------------------------------------
+// adjoint rows: inverse DFT along x, crop + shift, scale, deapodization,
+// conj(sens) coil sum
+// --------------------------------------------------------------------------
+// Per-coil outputs (stage 1, or no maps): one line per (row, coil), coil
+// fastest.
+template <int L>
+__global__ void __launch_bounds__(kFftThreads, L <= 256 ? 3 : 1)
+    k_fft_rows_adj_coils(const float2 *__restrict__ A,
+                         const float *__restrict__ deapo, int Nx,
+                         long long rows, long long N, int C, int out_add,
+                         float scale, int stage,
+                         const float2 *__restrict__ roots,
+                         float2 *__restrict__ out)
+{
+  using S = Shape<L>;
+  extern __shared__ float2 sm[];
+  float2 *tw = sm;
+  load_roots(tw, roots, L);
+  const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
+  const long long ln = (long long)blockIdx.x * S::NL + line;
+  const bool on = ln < rows * C;
+  const long long row = on ? ln / C : 0;
+  const int c = on ? (int)(ln - row * C) : 0;
+  float2 *Y = sm + L + line * S::R1 * S::YP;
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  if (lt < S::R2 && on)
+  {
+    const float2 *in = A + ((long long)c * rows + row) * L;
+    float2 a[S::R1];
+#pragma unroll
+    for (int j = 0; j < S::R1; ++j)
+      a[j] = __ldg(in + lt + S::R2 * j);
+    stage1<L, true, 1>(a, lt, w, tw, Y);
+  }
+  __syncthreads();
+  if (lt < S::R1 && on)
+  {
+    float2 b[S::R2];
+    stage2<L, true, 1>(b, lt, w, Y);
+#pragma unroll
+    for (int k2 = 0; k2 < S::R2; ++k2)
+    {
+      // FFT output k = lt + R1 k2 holds image x (k + out_add) mod L
+      const int xp = (lt + S::R1 * k2 + out_add) & (L - 1);
+      if (xp >= Nx)
+        continue;
+      const long long px = row * Nx + xp;
+      // crop -> FFT scaling -> deapodization (gpuNUFFT_operator.cpp:800-819)
+      float2 v = make_float2(__fmul_rn(b[k2].x, scale),
+                             __fmul_rn(b[k2].y, scale));
+      if (stage == 2)
+      {
+        const float d = __ldg(deapo + px);
+        v.x = __fmul_rn(v.x, d);
+        v.y = __fmul_rn(v.y, d);
+      }
+      out[c * N + px] = v;
+    }
+  }
+}
+
+// With maps (stage 2): the block owns RPB image rows and runs their coils
+// in chunks of CPC (lines = RPB x CPC); each chunk's conj(S) * v terms go
+// through shared memory and are added to the rows' running sums in coil
+// order, so the sum order is fixed.
+template <int L>
+__global__ void __launch_bounds__(kFftThreads, L <= 256 ? 3 : 1)
+    k_fft_rows_adj_sum(const float2 *__restrict__ A,
+                       const float *__restrict__ deapo,
+                       const float2 *__restrict__ sens, int Nx, long long rows,
+                       long long N, int C, int cpc, int out_add, float scale,
+                       int accumulate, const float2 *__restrict__ roots,
+                       float2 *__restrict__ out)
+{
+  using S = Shape<L>;
+  extern __shared__ float2 sm[];
+  float2 *tw = sm;
+  float2 *Ybase = sm + L;                       // exchange, then terms
+  float2 *accS = Ybase + S::NL * S::R1 * S::YP;  // [rpb][Nx] running sums
+  load_roots(tw, roots, L);
+  const int rpb = S::NL / cpc;
+  const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
+  const int rl = line / cpc, cl = line - rl * cpc;
+  const long long row = (long long)blockIdx.x * rpb + rl;
+  const bool row_on = row < rows;
+  float2 *Y = Ybase + line * S::R1 * S::YP;
+  float2 *term = Ybase + (size_t)line * Nx;  // aliases the exchange area
+  for (int i = threadIdx.x; i < rpb * Nx; i += kFftThreads)
+    accS[i] = make_float2(0.f, 0.f);
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  for (int c0 = 0; c0 < C; c0 += cpc)
+  {
+    const int c = c0 + cl;
+    const bool on = row_on && c < C;
+    if (lt < S::R2 && on)
+    {
+      const float2 *in = A + ((long long)c * rows + row) * L;
+      float2 a[S::R1];
+#pragma unroll
+      for (int j = 0; j < S::R1; ++j)
+        a[j] = __ldg(in + lt + S::R2 * j);
+      stage1<L, true, 1>(a, lt, w, tw, Y);
+    }
+    __syncthreads();
+    float2 b[S::R2];
+    if (lt < S::R1 && on)
+      stage2<L, true, 1>(b, lt, w, Y);
+    __syncthreads();  // the exchange area becomes the term area
+    if (lt < S::R1)
+    {
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int xp = (lt + S::R1 * k2 + out_add) & (L - 1);
+        if (xp >= Nx)
+          continue;
+        float2 t = make_float2(0.f, 0.f);
+        if (on)
+        {
+          const long long px = row * Nx + xp;
+          // crop -> FFT scaling -> deapodization -> conj(S) * v
+          // (gpuNUFFT_operator.cpp:800-843, std_gpuNUFFT_kernels.cu:158-218)
+          float2 v = make_float2(__fmul_rn(b[k2].x, scale),
+                                 __fmul_rn(b[k2].y, scale));
+          const float d = __ldg(deapo + px);
+          v.x = __fmul_rn(v.x, d);
+          v.y = __fmul_rn(v.y, d);
+          const float2 s = __ldg(sens + c * N + px);
+          t.x = v.x * s.x + v.y * s.y;
+          t.y = v.y * s.x - v.x * s.y;
+        }
+        term[xp] = t;
+      }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < rpb * Nx; i += kFftThreads)
+    {
+      const int r = i / Nx, x = i - r * Nx;
+      float2 sum = accS[i];
+      const int nc = min(cpc, C - c0);
+      for (int k = 0; k < nc; ++k)
+      {
+        const float2 t = Ybase[(size_t)(r * cpc + k) * Nx + x];
+        sum.x += t.x;
+        sum.y += t.y;
+      }
+      accS[i] = sum;
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < rpb * Nx; i += kFftThreads)
+  {
+    const int r = i / Nx, x = i - r * Nx;
+    const long long rr = (long long)blockIdx.x * rpb + r;
+    if (rr >= rows)
+      continue;
+    float2 v = accS[i];
+    if (accumulate)
+    {
+      const float2 o = out[rr * Nx + x];
+      v = make_float2(o.x + v.x, o.y + v.y);
+    }
+    out[rr * Nx + x] = v;
+  }
+}
+
+// --------------------------------------------------------------------------
+// dispatch
+// --------------------------------------------------------------------------
+inline int pos_mod(long long v, int m)
+{
+  long long r = v % m;
+  return (int)(r < 0 ? r + m : r);
+}
+
+template <class F> void with_length(int L, F &&f)
+{
+  switch (L)
+  {
+  case 16: f(std::integral_constant<int, 16>()); break;
+  case 32: f(std::integral_constant<int, 32>()); break;
+  case 64: f(std::integral_constant<int, 64>()); break;
+  case 128: f(std::integral_constant<int, 128>()); break;
+  case 256: f(std::integral_constant<int, 256>()); break;
+  case 512: f(std::integral_constant<int, 512>()); break;
+  case 1024: f(std::integral_constant<int, 1024>()); break;
+  default: throw Error(kInternal, "pruned transform length not supported");
+  }
+}
+
+template <class K> void set_smem(K kernel, size_t bytes)
+{
+  if (bytes > 48 * 1024)
+    GN_CUDA(cudaFuncSetAttribute(kernel,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)bytes));
+}
+
+template <bool INV>
+void cols(int L, const float2 *src, float2 *dst, long long ncols,
+          int src_rows, int dst_rows, long long planes, int in_add,
+          int in_count, int out_add, int out_count, const float2 *roots,
+          cudaStream_t s)
+{
+  with_length(L, [&](auto lc) {
+    constexpr int LL = decltype(lc)::value;
+    using S = Shape<LL>;
+    auto k = k_fft_cols<LL, INV>;
+    set_smem(k, S::col_smem());
+    if (planes > 65535)
+      throw Error(kNotSupported, "too many planes for the pruned transform");
+    const dim3 grid((unsigned)((ncols + S::TC - 1) / S::TC),
+                    (unsigned)planes);
+    k<<<grid, S::CT, S::col_smem(), s>>>(src, dst, ncols, src_rows,
+                                          dst_rows, in_add, in_count, out_add,
+                                          out_count, roots);
+    GN_LAUNCH_CHECK("pruned column transform");
+  });
+}
+
+}  // namespace
+
+bool pruned_fft_supported(const Geo &g)
+{
+  for (int a = 0; a < g.dim; ++a)
+  {
+    const int G = g.G[a];
+    if (G < 16 || G > 1024 || (G & (G - 1)))
+      return false;
+  }
+  return true;
+}
+
+void fft_roots(int L, std::vector<float2> &tab)
+{
+  tab.resize(L);
+  const double two_pi = 6.283185307179586476925286766559;
+  for (int j = 0; j < L; ++j)
+  {
+    const double ang = -two_pi * (double)j / (double)L;
+    tab[j] = make_float2((float)std::cos(ang), (float)std::sin(ang));
+  }
+}
+
+size_t pruned_scratch_a(const Geo &g, int C)
+{
+  return (size_t)C * g.N[2] * g.N[1] * g.G[0];
+}
+
+size_t pruned_scratch_b(const Geo &g, int C)
+{
+  return g.dim == 3 ? (size_t)C * g.N[2] * g.G[1] * g.G[0] : 0;
+}
+
+void launch_pruned_forward(const float2 *image, const float2 *sens,
+                           const float *deapo, const Geo &g, int C,
+                           const float2 *const roots[3], float2 *tmp_a,
+                           float2 *tmp_b, float2 *grid, cudaStream_t s)
+{
+  const long long N = g.img_count;
+  const long long rows = (long long)g.N[1] * g.N[2];
+  // x: image rows -> A [C][N_z][N_y][G_x]
+  with_length(g.G[0], [&](auto lc) {
+    constexpr int LL = decltype(lc)::value;
+    using S = Shape<LL>;
+    const long long nb = (rows * C + S::NL - 1) / S::NL;
+    const int in_add = pos_mod((long long)g.shift_inv[0] - g.crop[0], g.G[0]);
+    if (sens)
+    {
+      auto k = k_fft_rows_fwd<LL, true>;
+      set_smem(k, S::smem());
+      k<<<(unsigned)nb, kFftThreads, S::smem(), s>>>(
+          image, sens, deapo, g.N[0], rows, N, C, in_add, roots[0], tmp_a);
+    }
+    else
+    {
+      auto k = k_fft_rows_fwd<LL, false>;
+      set_smem(k, S::smem());
+      k<<<(unsigned)nb, kFftThreads, S::smem(), s>>>(
+          image, sens, deapo, g.N[0], rows, N, C, in_add, roots[0], tmp_a);
+    }
+    GN_LAUNCH_CHECK("pruned forward rows");
+  });
+  // y: A -> (3-D) B [C][N_z][G_y][G_x] or (2-D) the grid
+  float2 *ydst = g.dim == 3 ? tmp_b : grid;
+  cols<false>(g.G[1], tmp_a, ydst, g.G[0], g.N[1], g.G[1],
+              (long long)C * g.N[2],
+              pos_mod((long long)g.shift_inv[1] - g.crop[1], g.G[1]), g.N[1],
+              0, g.G[1], roots[1], s);
+  if (g.dim == 3)  // z: B -> grid
+    cols<false>(g.G[2], tmp_b, grid, (long long)g.G[1] * g.G[0], g.N[2],
+                g.G[2], C,
+                pos_mod((long long)g.shift_inv[2] - g.crop[2], g.G[2]),
+                g.N[2], 0, g.G[2], roots[2], s);
+}
+
+void launch_pruned_adjoint(const float2 *grid, const float *deapo,
+                           const float2 *sens, const Geo &g, int C, int stage,
+                           int accumulate, const float2 *const roots[3],
+                           float2 *tmp_a, float2 *tmp_b, float2 *out,
+                           cudaStream_t s)
+{
+  const long long N = g.img_count;
+  const long long rows = (long long)g.N[1] * g.N[2];
+  const float2 *ysrc = grid;
+  if (g.dim == 3)
+  {  // z: grid -> B [C][N_z][G_y][G_x]
+    cols<true>(g.G[2], grid, tmp_b, (long long)g.G[1] * g.G[0], g.G[2],
+               g.N[2], C, 0, g.G[2],
+               pos_mod(-(long long)g.crop[2] - g.shift_inv[2], g.G[2]),
+               g.N[2], roots[2], s);
+    ysrc = tmp_b;
+  }
+  // y: -> A [C][N_z][N_y][G_x]
+  cols<true>(g.G[1], ysrc, tmp_a, g.G[0], g.G[1], g.N[1],
+             (long long)C * g.N[2], 0, g.G[1],
+             pos_mod(-(long long)g.crop[1] - g.shift_inv[1], g.G[1]), g.N[1],
+             roots[1], s);
+  // x + image stages
+  with_length(g.G[0], [&](auto lc) {
+    constexpr int LL = decltype(lc)::value;
+    using S = Shape<LL>;
+    const int out_add =
+        pos_mod(-(long long)g.crop[0] - g.shift_inv[0], g.G[0]);
+    if (sens != nullptr && stage == 2)
+    {
+      int cpc = 1;
+      while (cpc < C && cpc < S::NL)
+        cpc <<= 1;
+      const int rpb = S::NL / cpc;
+      const size_t smem =
+          S::smem() + (size_t)rpb * g.N[0] * sizeof(float2);
+      auto k = k_fft_rows_adj_sum<LL>;
+      set_smem(k, smem);
+      k<<<(unsigned)((rows + rpb - 1) / rpb), kFftThreads, smem, s>>>(
+          tmp_a, deapo, sens, g.N[0], rows, N, C, cpc, out_add, g.fft_scale,
+          accumulate, roots[0], out);
+    }
+    else
+    {
+      auto k = k_fft_rows_adj_coils<LL>;
+      set_smem(k, S::smem());
+      k<<<(unsigned)((rows * C + S::NL - 1) / S::NL), kFftThreads, S::smem(),
+          s>>>(tmp_a, deapo, g.N[0], rows, N, C, out_add, g.fft_scale, stage,
+               roots[0], out);
+    }
+    GN_LAUNCH_CHECK("pruned adjoint rows");
+  });
+}
+
+}  // namespace gnufft

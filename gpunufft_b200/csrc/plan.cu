@@ -11,6 +11,7 @@
 // Calls restate GpuNUFFTOperator::performGpuNUFFTAdj / performForwardGpuNUFFT
 // (gpuNUFFT_operator.cpp:370-1294) with all coils of a call in one pass.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -26,6 +27,7 @@
 #include "../../include/gpunufft_b200.h"
 #include "binning.cuh"
 #include "devutil.hpp"
+#include "fftpass.cuh"
 #include "footprint.cuh"
 #include "geometry.hpp"
 #include "gridding.cuh"
@@ -71,6 +73,7 @@ struct gnufft_plan
   bool texture = false;
   bool plain = false;
   int fwd_tile_coils = 0;  // 0: automatic
+  bool pruned = false;     // separable pruned transforms instead of cuFFT
 
   // host copies of the exported tables
   std::vector<float> lut_h, traj_sorted_h, dens_sorted_h, deapo_h;
@@ -82,6 +85,7 @@ struct gnufft_plan
   DeviceBuffer adj_items, split_targets, fwd_items, deapo, sens;
   DeviceBuffer w_rows, w_nz;  // interpolation matrix, CSR by grid cell
   DeviceBuffer dlut;          // kernel derivative table (trajectory gradient)
+  DeviceBuffer roots[3];      // DFT roots per axis (pruned transforms)
   float dlut_mult = 0.f;
   size_t nnz = 0;
   int n_adj_items = 0, n_split = 0, n_fwd_items = 0;
@@ -90,7 +94,7 @@ struct gnufft_plan
   std::vector<float2> sens_h;
 
   // per-call scratch (grow-only)
-  DeviceBuffer ks, grid, stage_in, stage_out, one_sens;
+  DeviceBuffer ks, grid, stage_in, stage_out, one_sens, fft_a, fft_b;
   std::map<int, cufftHandle> fft;
 
   // timing
@@ -125,7 +129,9 @@ struct gnufft_plan
                                   &fwd_items,   &deapo,       &sens,
                                   &w_rows,      &w_nz,
                                   &ks,          &grid,        &stage_in,
-                                  &stage_out,   &one_sens};
+                                  &stage_out,   &one_sens,    &fft_a,
+                                  &fft_b,       &dlut,        &roots[0],
+                                  &roots[1],    &roots[2]};
     size_t s = 0;
     for (auto *b : bufs)
       s += b->bytes();
@@ -321,6 +327,8 @@ void init_common(gnufft_plan &p, const gnufft_desc *d)
     throw Error(kInvalidArgument, err);
   if (!gridding_supported(p.g, err))
     throw Error(kNotSupported, err);
+  p.pruned = !p.plain && !(d->flags & GNUFFT_FLAG_CUFFT) &&
+             pruned_fft_supported(p.g);
   p.dim = p.g.dim;
   p.M = d->n_samples;
   if ((size_t)p.M * (p.dim + 2) >= (1ull << 31))
@@ -522,6 +530,30 @@ void check_coils(const gnufft_plan &p, uint32_t C)
                 "n_coils differs from the sensitivity map channels");
 }
 
+// Root tables (once) and grow-only scratch of the pruned transforms.
+void ensure_pruned(gnufft_plan &p, uint32_t C, cudaStream_t s)
+{
+  for (int a = 0; a < p.g.dim; ++a)
+    if (!p.roots[a].get())
+    {
+      std::vector<float2> tab;
+      fft_roots(p.g.G[a], tab);
+      p.roots[a].reset(tab.size() * sizeof(float2));
+      GN_CUDA(cudaMemcpyAsync(p.roots[a].get(), tab.data(),
+                              tab.size() * sizeof(float2),
+                              cudaMemcpyHostToDevice, s));
+      GN_CUDA(cudaStreamSynchronize(s));
+    }
+  p.fft_a.ensure(pruned_scratch_a(p.g, (int)C) * sizeof(float2));
+  p.fft_b.ensure(pruned_scratch_b(p.g, (int)C) * sizeof(float2));
+}
+
+std::array<const float2 *, 3> root_ptrs(const gnufft_plan &p)
+{
+  return {p.roots[0].as<float2>(), p.roots[1].as<float2>(),
+          p.roots[2].as<float2>()};
+}
+
 // All coils of the call in one pass.
 void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
                      int stage, cudaStream_t s, const float2 *sens,
@@ -558,6 +590,20 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
     p.mark(7, s);
     return;
   }
+  if (p.pruned)
+  {  // inverse transform, crop, scale, deapodization and coil sum fused
+    ensure_pruned(p, C, s);
+    launch_pruned_adjoint(grid, p.deapo.as<float>(),
+                          stage == GNUFFT_DEAPODIZATION ? sens : nullptr, g,
+                          (int)C, stage == GNUFFT_FFT ? 1 : 2, accumulate,
+                          root_ptrs(p).data(), p.fft_a.as<float2>(),
+                          p.fft_b.as<float2>(), img, s);
+    p.launches += g.dim + 1;
+    p.mark(5, s);
+    p.mark(6, s);
+    p.mark(7, s);
+    return;
+  }
   cufftHandle h = p.fft_plan((int)C);
   check_cufft(cufftSetStream(h, s), "cufftSetStream");
   check_cufft(cufftExecC2C(h, (cufftComplex *)grid, (cufftComplex *)grid,
@@ -587,6 +633,29 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
   p.grid.ensure((size_t)C * g.grid_count * sizeof(float2));
   float2 *grid = p.grid.as<float2>();
   const bool dens_est = stage == GNUFFT_DENSITY_ESTIMATION;
+  if (p.pruned && !dens_est)
+  {  // sens, deapodization, pad, shift and the transform in g.dim passes
+    ensure_pruned(p, C, s);
+    p.mark(0, s);
+    p.mark(1, s);
+    p.mark(4, s);
+    launch_pruned_forward(img, sens, p.deapo.as<float>(), g, (int)C,
+                          root_ptrs(p).data(), p.fft_a.as<float2>(),
+                          p.fft_b.as<float2>(), grid, s);
+    p.launches += g.dim;
+    p.mark(5, s);
+    p.mark(2, s);
+    launch_forward_interp(
+        p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
+        p.di.as<uint32_t>(), p.has_dens ? p.dens_sorted.as<float>() : nullptr,
+        grid, g, p.lut.as<float>(), p.M, (int)C, true, g.fft_scale, k, s,
+        p.fwd_tile_coils);
+    p.launches += 1;
+    p.mark(3, s);
+    p.mark(6, s);
+    p.mark(7, s);
+    return;
+  }
   p.mark(0, s);
   launch_forward_prepare(img, sens, p.deapo.as<float>(), g, (int)C, dens_est,
                          grid, s);

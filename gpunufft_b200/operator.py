@@ -53,7 +53,7 @@ class Plan:
                  sens=None, operator_type: int = C.BALANCED,
                  reference_order: bool = False, plain: bool = False,
                  device: int = 0, tile_coils: int = 0,
-                 _load: Optional[dict] = None):
+                 use_cufft: bool = False, _load: Optional[dict] = None):
         self._h = ctypes.c_void_p()
         dims = [int(v) for v in img_dims]
         if len(dims) == 2:
@@ -88,6 +88,7 @@ class Plan:
         d.operator_type = int(operator_type)
         d.flags = ((C.FLAG_REFERENCE_ORDER if reference_order else 0) |
                    (C.FLAG_PLAIN if plain else 0) |
+                   (C.FLAG_CUFFT if use_cufft else 0) |
                    C.fwd_tile_flag(tile_coils))
         d.device = int(device)
         self.device = int(device)

@@ -98,6 +98,11 @@ typedef enum gnufft_output {
  * coil.  For comparisons only; the default executes all coils of a call in
  * one pass with resident maps. */
 #define GNUFFT_FLAG_PLAIN 0x2u
+/* Run the Cartesian transforms through cuFFT (the full 3 passes over the
+ * oversampled grid) instead of the separable pruned transforms fused with the
+ * image-space stages, which are the default when every grid axis is a power
+ * of two in [16, 1024].  For comparisons. */
+#define GNUFFT_FLAG_CUFFT 0x4u
 /* Forward-interpolation tile shape (the autotuner's knob): coils staged per
  * sector tile, n = 1, 2, 4, 8, 16 or 32, stored in bits 8-11 as
  * log2(n) + 1; 0 selects automatically.  n is reduced until the tile fits
