@@ -565,7 +565,7 @@ __global__ void k_zero_targets(const int *__restrict__ targets, Geo g, int C,
 constexpr int kSpmmCells = 64;
 
 template <int CG>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 3)
     k_adjoint_spmm(const uint32_t *__restrict__ row_off,
                    const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
                    int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
@@ -640,53 +640,69 @@ __global__ void __launch_bounds__(kThreads, 4)
   {
     uint32_t bound = s_off[cell + 1];
     float ax = 0.f, ay = 0.f;
-    uint2 qn[B];
-#pragma unroll
-    for (int u = 0; u < B; ++u)
-      qn[u] = (u0 + u < u1) ? __ldg(nz + u0 + u) : make_uint2(0u, 0u);
-    for (uint32_t k0 = u0; k0 < u1; k0 += B)
+    // a cell boundary: the finished cell lies inside this share (store) or
+    // started in an earlier share (head partial)
+#define GN_SPMM_FLUSH(KK)                                                      \
+  while ((KK) >= bound)                                                        \
+  {                                                                            \
+    if (s_off[cell] < u0)                                                      \
+    {                                                                          \
+      part_head[unit][coil] = make_float2(ax, ay);                             \
+      if (coil == 0)                                                           \
+        head_cell[unit] = cell;                                                \
+    }                                                                          \
+    else                                                                       \
+      acc_s[cell][coil] = make_float2(ax, ay);                                 \
+    ax = ay = 0.f;                                                             \
+    ++cell;                                                                    \
+    bound = s_off[cell + 1];                                                   \
+  }
+    // whole batches of B entries: the next batch's (sample, weight) pairs
+    // load while this batch's k-space rows are read
+    const uint32_t kfull = u0 + (u1 - u0) / B * B;
+    uint32_t k0 = u0;
+    if (k0 < kfull)
     {
       uint2 q[B];
 #pragma unroll
       for (int u = 0; u < B; ++u)
-        q[u] = qn[u];
-      const bool full = k0 + B <= u1;
-      // prefetch the next batch of (sample, weight) pairs
-#pragma unroll
-      for (int u = 0; u < B; ++u)
-        qn[u] = (k0 + B + u < u1) ? __ldg(nz + k0 + B + u)
-                                  : make_uint2(0u, 0u);
-      float2 v[B];
-#pragma unroll
-      for (int u = 0; u < B; ++u)
-        v[u] = (full || k0 + u < u1) ? __ldg(ksg + (size_t)q[u].x * CP)
-                                     : make_float2(0.f, 0.f);
-      const uint32_t nb = full ? B : u1 - k0;
-#pragma unroll
-      for (int u = 0; u < B; ++u)
+        q[u] = __ldg(nz + k0 + u);
+      for (; k0 < kfull; k0 += B)
       {
-        if ((uint32_t)u >= nb)
-          break;
-        const uint32_t k = k0 + u;
-        while (k >= bound)
-        {  // cell boundary: the cell is complete within this share
-          if (s_off[cell] < u0)
-          {
-            part_head[unit][coil] = make_float2(ax, ay);
-            if (coil == 0)
-              head_cell[unit] = cell;
-          }
-          else
-            acc_s[cell][coil] = make_float2(ax, ay);
-          ax = ay = 0.f;
-          ++cell;
-          bound = s_off[cell + 1];
+        float2 v[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+          v[u] = __ldg(ksg + q[u].x * (uint32_t)CP);
+        uint2 qn[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+        {  // clamped: always a valid entry of this share
+          const uint32_t kn = k0 + B + u;
+          qn[u] = __ldg(nz + (kn < u1 ? kn : u1 - 1));
         }
-        const float w = __uint_as_float(q[u].y);
-        ax = __fmaf_rn(w, v[u].x, ax);
-        ay = __fmaf_rn(w, v[u].y, ay);
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+        {
+          GN_SPMM_FLUSH(k0 + u)
+          const float w = __uint_as_float(q[u].y);
+          ax = __fmaf_rn(w, v[u].x, ax);
+          ay = __fmaf_rn(w, v[u].y, ay);
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+          q[u] = qn[u];
       }
     }
+    for (; k0 < u1; ++k0)
+    {  // the remainder, one entry at a time
+      const uint2 q = __ldg(nz + k0);
+      const float2 v = __ldg(ksg + q.x * (uint32_t)CP);
+      GN_SPMM_FLUSH(k0)
+      const float w = __uint_as_float(q.y);
+      ax = __fmaf_rn(w, v.x, ax);
+      ay = __fmaf_rn(w, v.y, ay);
+    }
+#undef GN_SPMM_FLUSH
     if (s_off[cell] < u0)
     {
       part_head[unit][coil] = make_float2(ax, ay);

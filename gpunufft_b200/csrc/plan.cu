@@ -562,6 +562,8 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
   const Geo &g = p.g;
   const int cg = spmm_coil_group((int)C);
   const int CP = ((int)C + cg - 1) / cg * cg;
+  if ((size_t)p.M * CP > 0xFFFFFFFFull)  // 32-bit row offsets in the spread
+    throw Error(kNotSupported, "samples x coil lanes exceed 2^32");
   p.ks.ensure((size_t)p.M * CP * sizeof(float2));
   const bool conv = stage == GNUFFT_CONVOLUTION ||
                     stage == GNUFFT_DENSITY_ESTIMATION;
