@@ -303,6 +303,24 @@ def profile_traffic(name, kernel):
         return None
 
 
+def reduce_over_ranks(value, dist, device, op="max"):
+    """The max (or min) of a per-rank float over all ranks (identity when
+    there is no process group).  Every rank takes part, in the same order."""
+    if dist is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max"
+                    else dist.ReduceOp.MIN)
+    return float(t.item())
+
+
+def replica_throughput(steps, world, ms_max):
+    """Whole-job steps per second: every replica runs ``steps``; the job
+    takes as long as the slowest rank."""
+    return world * steps / (ms_max / 1e3)
+
+
 def run_gpu_arm(args, rank, world, dist):
     import torch
     import gpunufft_b200 as G
@@ -339,13 +357,9 @@ def run_gpu_arm(args, rank, world, dist):
         ev1.record(stream)
         torch.cuda.synchronize()
     barrier()
-    ms = ev0.elapsed_time(ev1)
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     ms_per_step = ms / args.steps
-    value = world * args.steps / (ms / 1e3)
+    value = replica_throughput(args.steps, world, ms)
 
     # stage times (CUDA events on the plan's launch stream), timed steps
     plan.set_timing(True)
@@ -414,12 +428,8 @@ def run_gpu_arm(args, rank, world, dist):
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = world * args.steps / (e2e_ms / 1e3)
+    e2e_ms = reduce_over_ranks(e0.elapsed_time(e1), dist, dev)
+    e2e_value = replica_throughput(args.steps, world, e2e_ms)
     h2d = xh.numel() * 8 + kh.numel() * 8
     d2h = out_k.numel() * 8 + out_x.numel() * 8
 
@@ -439,10 +449,8 @@ def run_gpu_arm(args, rank, world, dist):
         torch.cuda.synchronize()
         plain_value = args.plain_steps / (time.perf_counter() - p0)
         plan_p.close()
-        if dist is not None:
-            t = torch.tensor([plain_value], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MIN)
-            plain_value = float(t.item()) * world
+        plain_value = reduce_over_ranks(plain_value, dist, dev,
+                                        "min") * world
 
     # the upstream library's own GPU operator, built from its sources for
     # sm_100a (oracle/_ref), on the same inputs through its host-array API
