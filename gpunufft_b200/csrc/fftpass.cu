@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kFftThreads, L <= 256 ? 3 : 1)
     k_fft_rows_fwd(const float2 *__restrict__ image,
                    const float2 *__restrict__ sens,
                    const float *__restrict__ deapo, int Nx, long long rows,
-                   long long N, int C, int in_add,
+                   long long N, int C, int in_add, int out_add,
                    const float2 *__restrict__ roots, float2 *__restrict__ A)
 {
   using S = Shape<L>;
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(kFftThreads, L <= 256 ? 3 : 1)
     float2 *out = A + ((long long)c * rows + row) * L;
 #pragma unroll
     for (int k2 = 0; k2 < S::R2; ++k2)
-      out[lt + S::R1 * k2] = b[k2];
+      out[(lt + S::R1 * k2 + out_add) & (L - 1)] = b[k2];
   }
 }
 
@@ -576,19 +576,23 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
     using S = Shape<LL>;
     const long long nb = (rows * C + S::NL - 1) / S::NL;
     const int in_add = pos_mod((long long)g.shift_inv[0] - g.crop[0], g.G[0]);
+    // the FORWARD fftshift: frequency k is stored at (k - ceil(G/2)) mod G
+    const int out_add = pos_mod(-(long long)g.shift_fwd[0], g.G[0]);
     if (sens)
     {
       auto k = k_fft_rows_fwd<LL, true>;
       set_smem(k, S::smem());
       k<<<(unsigned)nb, kFftThreads, S::smem(), s>>>(
-          image, sens, deapo, g.N[0], rows, N, C, in_add, roots[0], tmp_a);
+          image, sens, deapo, g.N[0], rows, N, C, in_add, out_add, roots[0],
+          tmp_a);
     }
     else
     {
       auto k = k_fft_rows_fwd<LL, false>;
       set_smem(k, S::smem());
       k<<<(unsigned)nb, kFftThreads, S::smem(), s>>>(
-          image, sens, deapo, g.N[0], rows, N, C, in_add, roots[0], tmp_a);
+          image, sens, deapo, g.N[0], rows, N, C, in_add, out_add, roots[0],
+          tmp_a);
     }
     GN_LAUNCH_CHECK("pruned forward rows");
   });
@@ -597,12 +601,14 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
   cols<false>(g.G[1], tmp_a, ydst, g.G[0], g.N[1], g.G[1],
               (long long)C * g.N[2],
               pos_mod((long long)g.shift_inv[1] - g.crop[1], g.G[1]), g.N[1],
-              0, g.G[1], roots[1], s);
+              pos_mod(-(long long)g.shift_fwd[1], g.G[1]), g.G[1], roots[1],
+              s);
   if (g.dim == 3)  // z: B -> grid
     cols<false>(g.G[2], tmp_b, grid, (long long)g.G[1] * g.G[0], g.N[2],
                 g.G[2], C,
                 pos_mod((long long)g.shift_inv[2] - g.crop[2], g.G[2]),
-                g.N[2], 0, g.G[2], roots[2], s);
+                g.N[2], pos_mod(-(long long)g.shift_fwd[2], g.G[2]), g.G[2],
+                roots[2], s);
 }
 
 void launch_pruned_adjoint(const float2 *grid, const float *deapo,

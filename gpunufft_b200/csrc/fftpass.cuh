@@ -40,7 +40,8 @@ size_t pruned_scratch_b(const Geo &g, int C);
 
 // Forward: image ([N] with maps, else [C][N]) -> sens multiply ->
 // deapodization -> zero pad -> INVERSE fftshift -> unnormalised forward DFT
-// -> grid [C][G]: the array cuFFT FORWARD produces from the prepared grid.
+// -> FORWARD fftshift -> grid [C][G] (so cell q of the shifted spectrum, the
+// one the interpolation reads, is stored at q).
 // roots[a]: the root table of axis a (length G[a]).
 void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,

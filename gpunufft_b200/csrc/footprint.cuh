@@ -57,6 +57,14 @@ GN_HD uint32_t sector_of_axis(float c, float G, float sw)
   return (uint32_t)s;
 }
 
+// gc / G in float (mapGridToKSpace, gpuNUFFT_utils.hpp:202-209); for a
+// power-of-two G the product with the exact reciprocal is the same number.
+GN_HD float grid_to_k(int gc, int ax, const Geo &g)
+{
+  return g.pow2G[ax] ? GN_FMUL((float)gc, g.invG[ax])
+                     : GN_FDIV((float)gc, g.Gf[ax]);
+}
+
 // Linear interpolation of a table over normalised coordinate u, the way the
 // texture unit filters a normalised, clamp-addressed texture: texel
 // coordinate u*W - 0.5, weight quantised to 8 fractional bits
@@ -115,7 +123,7 @@ GN_HD int axis_footprint(float c, int ax, int sector_ax, const Geo &g,
   for (int i = imin; i <= imax; ++i)
   {
     int gc = i + center - g.offset;
-    float k = GN_FSUB(GN_FDIV((float)gc, g.Gf[ax]), 0.5f);
+    float k = GN_FSUB(grid_to_k(gc, ax, g), 0.5f);
     float d = GN_FMUL(GN_FSUB(k, c), g.aniso[ax]);
     float d2 = GN_FMUL(d, d);
     float wt;

@@ -135,6 +135,8 @@ bool make_geo(const uint32_t img[3], float osf, uint32_t kw, uint32_t sw,
     g.S[a] = used ? (int)std::ceil(static_cast<float>(grid[a]) / sw) : 1;
     g.Gf[a] = (float)g.G[a];
     g.halfG[a] = 0.5f * g.Gf[a];
+    g.pow2G[a] = g.G[a] > 0 && (g.G[a] & (g.G[a] - 1)) == 0;
+    g.invG[a] = g.pow2G[a] ? 1.0f / g.Gf[a] : 0.0f;
     gc *= g.G[a];
     ic *= g.N[a];
   }

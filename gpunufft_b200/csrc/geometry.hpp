@@ -34,6 +34,9 @@ struct Geo
   int sw, kw, pad, offset;
   float Gf[3];      // (float)G
   float halfG[3];   // 0.5f * (float)G
+  float invG[3];    // 1 / G, used instead of a division when G is a power
+                    // of two (then x * (1/G) == x / G exactly)
+  int pow2G[3];     // G is a power of two
   float kernel_radius;   // kw / 2
   float radius_sq;       // (kw/2 / max G)^2, stored float (double math)
   float radius_sq_inv;

@@ -21,6 +21,8 @@
 
 #include <algorithm>
 
+#include <cuda.h>
+
 #include "devutil.hpp"
 #include "footprint.cuh"
 
@@ -158,7 +160,7 @@ __device__ __forceinline__ int compact_axis(float c, int ax, int sec_ax,
   {
     const int i = imin + k;
     const int gc = i + center - g.offset;
-    const float kx = __fsub_rn(__fdiv_rn((float)gc, g.Gf[ax]), 0.5f);
+    const float kx = __fsub_rn(grid_to_k(gc, ax, g), 0.5f);
     const float d = __fmul_rn(__fsub_rn(kx, c), g.aniso[ax]);
     const float d2 = __fmul_rn(d, d);
     bool valid = i <= imax && i >= 0;
@@ -938,6 +940,200 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // --------------------------------------------------------------------------
+// forward interpolation, tile by TMA (the grid holds the FORWARD-shifted
+// spectrum, so a sector tile is one box of the grid unless it wraps)
+// --------------------------------------------------------------------------
+// Shared memory: tile [CG][PZ][PY][PX] (x fastest; PX = pad + 1 rounded up
+// to even, so that the box starts on an even x, i.e. a 16-byte boundary)
+// and one mbarrier.  Thread 0 issues one bulk tensor copy of the box at
+// (x0, y0, z0, first coil); tiles that wrap around the grid edge are
+// gathered with plain loads instead.  Then every thread takes one sample:
+// its per-axis footprint (tile frame, upstream arithmetic) in registers,
+// and for each footprint cell the CG coil values of the tile.
+constexpr long long kMbarSpin = 1LL << 22;  // bounded wait for the copy
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p)
+{
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+template <int DIM, int CG, int KS>
+__global__ void __launch_bounds__(kThreads)
+    k_forward_tma(const __grid_constant__ CUtensorMap tmap,
+                  const FwdItem *__restrict__ items,
+                  const float *__restrict__ traj,
+                  const uint32_t *__restrict__ idx,
+                  const float *__restrict__ dens,
+                  const float2 *__restrict__ grid, Geo g,
+                  const float *__restrict__ lut, uint32_t M, int C, int PX,
+                  float scale, float2 *__restrict__ out,
+                  int *__restrict__ err)
+{
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int pad = g.pad;
+  const int PY = pad, PZ = DIM == 3 ? pad : 1;
+  const int cstride = PZ * PY * PX;  // elements per coil
+  float2 *tile = reinterpret_cast<float2 *>(smraw);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(
+      smraw + (size_t)CG * cstride * sizeof(float2));
+  int &s_fail = *reinterpret_cast<int *>(mbar + 1);
+  const FwdItem it = items[blockIdx.x];
+  const int c0 = blockIdx.y * CG;
+  int sa[3];
+  split_sector(it.sector, g, sa);
+  int base[3] = {0, 0, 0};
+  for (int a = 0; a < DIM; ++a)
+    base[a] = sa[a] * g.sw + (g.sw >> 1) - g.offset;
+  const int x0 = base[0] & ~1;  // even start (floor, negative included)
+  const int dx = base[0] - x0;
+  bool inside = true;
+  for (int a = 0; a < DIM; ++a)
+    inside = inside && base[a] >= 0 && base[a] + pad <= g.G[a];
+  if (inside)
+  {
+    const uint32_t bar = smem_addr(mbar);
+    if (threadIdx.x == 0)
+    {
+      s_fail = 0;
+      const uint32_t bytes = (uint32_t)(CG * cstride * sizeof(float2));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar)
+                   : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile(
+          "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+          "r"(bytes)
+          : "memory");
+      const uint32_t dst = smem_addr(tile);
+      const uint64_t tm = reinterpret_cast<uint64_t>(&tmap);
+      if (DIM == 3)
+        asm volatile(
+            "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::"
+            "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+            "l"(tm), "r"(x0), "r"(base[1]), "r"(base[2]), "r"(c0), "r"(bar)
+            : "memory");
+      else
+        asm volatile(
+            "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::"
+            "complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+            "l"(tm), "r"(x0), "r"(base[1]), "r"(c0), "r"(bar)
+            : "memory");
+    }
+    __syncthreads();
+    uint32_t done = 0;
+    for (long long i = 0; i < kMbarSpin && !done; ++i)
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], "
+          "0; selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(bar)
+          : "memory");
+    if (!done)
+      s_fail = 1;
+    __syncthreads();
+    if (s_fail)
+    {  // the copy did not complete: report, do not use the tile
+      if (threadIdx.x == 0)
+        atomicExch(err, 1);
+      return;
+    }
+  }
+  else
+  {  // a tile that wraps around the grid edge: plain loads
+    const long long G = g.grid_count;
+    for (int e = threadIdx.x; e < CG * cstride; e += kThreads)
+    {
+      const int c = e / cstride;
+      int r = e - c * cstride;
+      const int z = r / (PY * PX);
+      r -= z * PY * PX;
+      const int y = r / PX, x = r - y * PX;
+      float2 v = make_float2(0.f, 0.f);
+      if (c0 + c < C)
+      {
+        int q[3] = {x0 + x, base[1] + y, DIM == 3 ? base[2] + z : 0};
+        for (int a = 0; a < DIM; ++a)
+          q[a] = ((q[a] % g.G[a]) + g.G[a]) % g.G[a];
+        v = __ldg(grid + (long long)(c0 + c) * G +
+                  ((long long)q[2] * g.G[1] + q[1]) * g.G[0] + q[0]);
+      }
+      tile[e] = v;
+    }
+    __syncthreads();
+  }
+
+  for (int t = it.begin + threadIdx.x; t < it.end; t += kThreads)
+  {
+    int l[3][KS];
+    float w[3][KS];
+    int n[3] = {1, 1, 1};
+    l[2][0] = 0;
+    w[2][0] = 1.f;
+#pragma unroll
+    for (int a = 0; a < DIM; ++a)
+      n[a] = compact_axis<KS>(__ldg(traj + (size_t)a * M + t), a, sa[a], 0, g,
+                              lut, false, l[a], w[a]);
+    float2 acc[CG];
+#pragma unroll
+    for (int c = 0; c < CG; ++c)
+      acc[c] = make_float2(0.f, 0.f);
+    // tile-frame entries are consecutive cells starting at l[a][0]
+    const int xb = l[0][0] + dx;
+    for (int z = 0; z < n[2]; ++z)
+    {
+      float wzv = 1.f;
+#pragma unroll
+      for (int k = 0; k < KS; ++k)
+        if (k == z)
+          wzv = w[2][k];
+      for (int y = 0; y < n[1]; ++y)
+      {
+        float wyv = 0.f;
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
+          if (k == y)
+            wyv = w[1][k];
+        const float wzy = DIM == 3 ? __fmul_rn(wzv, wyv) : wyv;
+        const int row = ((DIM == 3 ? (l[2][0] + z) * PY : 0) + l[1][0] + y) *
+                            PX + xb;
+#pragma unroll
+        for (int x = 0; x < KS; ++x)
+        {
+          if (x < n[0])
+          {
+            const float wt = __fmul_rn(wzy, w[0][x]);
+#pragma unroll
+            for (int c = 0; c < CG; ++c)
+            {
+              const float2 v = tile[c * cstride + row + x];
+              acc[c].x = __fmaf_rn(v.x, wt, acc[c].x);
+              acc[c].y = __fmaf_rn(v.y, wt, acc[c].y);
+            }
+          }
+        }
+      }
+    }
+    const uint32_t j = __ldg(idx + t);
+    const float sd = dens ? sqrtf(__ldg(dens + t)) : 1.0f;
+#pragma unroll
+    for (int c = 0; c < CG; ++c)
+    {
+      if (c0 + c < C)
+      {
+        // performFFTScaling then performDensityCompensation
+        // (std_gpuNUFFT_kernels.cu:114-140, 220-242)
+        float ax = __fmul_rn(acc[c].x, scale), ay = __fmul_rn(acc[c].y, scale);
+        if (dens)
+        {
+          ax = __fmul_rn(ax, sd);
+          ay = __fmul_rn(ay, sd);
+        }
+        out[(size_t)(c0 + c) * M + j] = make_float2(ax, ay);
+      }
+    }
+  }
+}
+
+// --------------------------------------------------------------------------
 // image-space stages
 // --------------------------------------------------------------------------
 template <bool SENS>
@@ -1414,6 +1610,134 @@ void launch_forward_interp(const FwdItem *items, int n_items,
   }
 #undef GN_FWD_CG
 #undef GN_FWD
+}
+
+
+// Tensor-map encoding through the driver entry point (no link-time
+// dependency on the driver library).
+namespace
+{
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType,
+                                  cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *,
+                                  const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion,
+                                  CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+  static EncodeTiledFn fn = [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f,
+                                cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (EncodeTiledFn) nullptr;
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+}  // namespace
+
+bool launch_forward_interp_tma(const FwdItem *items, int n_items,
+                               const float *traj_sorted, const uint32_t *idx,
+                               const float *dens_sorted, const float2 *grid,
+                               const Geo &g, const float *lut, uint32_t M,
+                               int C, float scale, float2 *out, int *err,
+                               cudaStream_t s, int tile_coils)
+{
+  if (n_items <= 0)
+    return true;
+  EncodeTiledFn enc = encode_fn();
+  if (!enc || (g.G[0] & 1))
+    return false;
+  const int pad = g.pad;
+  const int PX = (pad + 2) & ~1;  // pad + 1 rounded up to even
+  // coils per tile: a power of two, at most C (the box stays inside the
+  // coil extent) and at most 4 in 3-D (64 KB tiles, three blocks per SM)
+  const int cmax = std::min(C, tile_coils > 0
+                                   ? std::min(tile_coils, g.dim == 3 ? 4 : 32)
+                                   : (g.dim == 3 ? 4 : 32));
+  int cg = 1;
+  while (cg * 2 <= cmax)
+    cg <<= 1;
+  const int PZ = g.dim == 3 ? pad : 1;
+  const size_t tile = (size_t)cg * PZ * pad * PX * sizeof(float2);
+  const size_t smem = tile + 16;
+  if (smem > 200 * 1024 || PX > 256 || pad > 256)
+    return false;
+  CUtensorMap tm;
+  cuuint64_t dims[4], strides[3];
+  cuuint32_t box[4], estr[4] = {1, 1, 1, 1};
+  const int rank = g.dim + 1;
+  dims[0] = g.G[0];
+  dims[1] = g.G[1];
+  strides[0] = (cuuint64_t)g.G[0] * sizeof(float2);
+  box[0] = PX;
+  box[1] = pad;
+  if (g.dim == 3)
+  {
+    dims[2] = g.G[2];
+    dims[3] = C;
+    strides[1] = strides[0] * g.G[1];
+    strides[2] = strides[1] * g.G[2];
+    box[2] = pad;
+    box[3] = cg;
+  }
+  else
+  {
+    dims[2] = C;
+    strides[1] = strides[0] * g.G[1];
+    box[2] = cg;
+  }
+  if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, rank,
+          const_cast<float2 *>(grid), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  const dim3 grd((unsigned)n_items, (unsigned)((C + cg - 1) / cg));
+  const int ks = slots_for(g);
+#define GN_TMA(D, CGV, KSV)                                                    \
+  {                                                                            \
+    auto k = k_forward_tma<D, CGV, KSV>;                                       \
+    if (smem > 48 * 1024)                                                      \
+      GN_CUDA(cudaFuncSetAttribute(                                            \
+          k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));         \
+    k<<<grd, kThreads, smem, s>>>(tm, items, traj_sorted, idx, dens_sorted,    \
+                                  grid, g, lut, M, C, PX, scale, out, err);    \
+  }
+#define GN_TMA_KS(D, CGV)                                                      \
+  if (ks == 4)                                                                 \
+    GN_TMA(D, CGV, 4)                                                          \
+  else                                                                         \
+    GN_TMA(D, CGV, 8)
+  if (g.dim == 3)
+  {
+    switch (cg)
+    {
+    case 1: GN_TMA_KS(3, 1); break;
+    case 2: GN_TMA_KS(3, 2); break;
+    default: GN_TMA_KS(3, 4); break;
+    }
+  }
+  else
+  {
+    switch (cg)
+    {
+    case 1: GN_TMA_KS(2, 1); break;
+    case 2: GN_TMA_KS(2, 2); break;
+    case 4: GN_TMA_KS(2, 4); break;
+    case 8: GN_TMA_KS(2, 8); break;
+    case 16: GN_TMA_KS(2, 16); break;
+    default: GN_TMA_KS(2, 32); break;
+    }
+  }
+#undef GN_TMA_KS
+#undef GN_TMA
+  GN_LAUNCH_CHECK("forward interpolation (tensor-copy tiles)");
+  return true;
 }
 
 }  // namespace gnufft

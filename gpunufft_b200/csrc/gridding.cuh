@@ -98,4 +98,17 @@ void launch_forward_interp(const FwdItem *items, int n_items,
                            bool shift, float scale, float2 *out,
                            cudaStream_t s, int tile_coils = 0);
 
+// Forward interpolation with each sector tile fetched by one bulk tensor
+// copy (tiles that wrap around the grid edge by plain loads).  The grid
+// must hold the FORWARD-shifted spectrum (cell q at q).  `err` (device
+// pointer) is set to 1 if a copy did not complete within the bounded wait.
+// Returns false when the geometry does not suit tensor copies (nothing is
+// launched then).
+bool launch_forward_interp_tma(const FwdItem *items, int n_items,
+                               const float *traj_sorted, const uint32_t *idx,
+                               const float *dens_sorted, const float2 *grid,
+                               const Geo &g, const float *lut, uint32_t M,
+                               int C, float scale, float2 *out, int *err,
+                               cudaStream_t s, int tile_coils = 0);
+
 }  // namespace gnufft

@@ -74,6 +74,8 @@ struct gnufft_plan
   bool plain = false;
   int fwd_tile_coils = 0;  // 0: automatic
   bool pruned = false;     // separable pruned transforms instead of cuFFT
+  int *copy_err_h = nullptr;  // set by a tile copy that timed out (mapped)
+  int *copy_err_d = nullptr;
 
   // host copies of the exported tables
   std::vector<float> lut_h, traj_sorted_h, dens_sorted_h, deapo_h;
@@ -117,6 +119,8 @@ struct gnufft_plan
         cudaEventDestroy(e);
     if (stream)
       cudaStreamDestroy(stream);
+    if (copy_err_h)
+      cudaFreeHost(copy_err_h);
     if (prev >= 0)
       cudaSetDevice(prev);
   }
@@ -329,6 +333,14 @@ void init_common(gnufft_plan &p, const gnufft_desc *d)
     throw Error(kNotSupported, err);
   p.pruned = !p.plain && !(d->flags & GNUFFT_FLAG_CUFFT) &&
              pruned_fft_supported(p.g);
+  if (p.pruned)
+  {
+    GN_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&p.copy_err_h),
+                          sizeof(int), cudaHostAllocMapped));
+    *p.copy_err_h = 0;
+    GN_CUDA(cudaHostGetDevicePointer(reinterpret_cast<void **>(&p.copy_err_d),
+                                     p.copy_err_h, 0));
+  }
   p.dim = p.g.dim;
   p.M = d->n_samples;
   if ((size_t)p.M * (p.dim + 2) >= (1ull << 31))
@@ -637,6 +649,12 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
   const bool dens_est = stage == GNUFFT_DENSITY_ESTIMATION;
   if (p.pruned && !dens_est)
   {  // sens, deapodization, pad, shift and the transform in g.dim passes
+    if (*(volatile int *)p.copy_err_h)
+    {
+      *p.copy_err_h = 0;
+      throw Error(kCudaError,
+                  "a forward tile copy did not complete within its wait");
+    }
     ensure_pruned(p, C, s);
     p.mark(0, s);
     p.mark(1, s);
@@ -647,11 +665,19 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
     p.launches += g.dim;
     p.mark(5, s);
     p.mark(2, s);
-    launch_forward_interp(
-        p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
-        p.di.as<uint32_t>(), p.has_dens ? p.dens_sorted.as<float>() : nullptr,
-        grid, g, p.lut.as<float>(), p.M, (int)C, true, g.fft_scale, k, s,
-        p.fwd_tile_coils);
+    // the grid holds the shifted spectrum: sector tiles are boxes of it
+    if (!launch_forward_interp_tma(
+            p.fwd_items.as<FwdItem>(), p.n_fwd_items,
+            p.traj_sorted.as<float>(), p.di.as<uint32_t>(),
+            p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
+            p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, p.copy_err_d, s,
+            p.fwd_tile_coils))
+      launch_forward_interp(
+          p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
+          p.di.as<uint32_t>(),
+          p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
+          p.lut.as<float>(), p.M, (int)C, false, g.fft_scale, k, s,
+          p.fwd_tile_coils);
     p.launches += 1;
     p.mark(3, s);
     p.mark(6, s);

@@ -86,7 +86,7 @@ __global__ void __launch_bounds__(kGradThreads)
       for (int e = 0; e < n[a]; ++e)
       {
         const int gc = loc[e] + center - g.offset;
-        const float k = __fsub_rn(__fdiv_rn((float)gc, g.Gf[a]), 0.5f);
+        const float k = __fsub_rn(grid_to_k(gc, a, g), 0.5f);
         const float d = __fmul_rn(__fsub_rn(k, c), g.aniso[a]);
         const float d2 = __fmul_rn(d, d);
         dw[a][e] = d2 < g.radius_sq
