@@ -566,15 +566,18 @@ __global__ void k_zero_targets(const int *__restrict__ targets, Geo g, int C,
 // (INVERSE fftshift folded into the store position).
 constexpr int kSpmmCells = 64;
 
-template <int CG>
+// V coils per lane (V = 2 reads a lane's two coils as one 16-byte load and
+// halves the per-entry instructions per coil).
+template <int CG, int V>
 __global__ void __launch_bounds__(kThreads, 3)
     k_adjoint_spmm(const uint32_t *__restrict__ row_off,
                    const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
                    int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
 {
-  constexpr int SLOTS = 32 / CG;
+  constexpr int LS = CG / V;          // lanes per slot
+  constexpr int SLOTS = 32 / LS;
   constexpr int NU = kWarps * SLOTS;  // streaming units per block
-  constexpr int B = 8;                // entries per batch
+  constexpr int B = 8 / V;            // entries per batch
   __shared__ float2 acc_s[kSpmmCells][CG + 1];
   __shared__ uint32_t s_off[kSpmmCells + 1];
   // partial sums of cells cut by share boundaries: head = the unit's first
@@ -621,9 +624,9 @@ __global__ void __launch_bounds__(kThreads, 3)
   __syncthreads();
 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slot = lane / CG, coil = lane % CG;
+  const int slot = lane / LS, cl = lane % LS;
   const int unit = warp * SLOTS + slot;
-  const float2 *ksg = ks + group * CG + coil;
+  const float2 *ksg = ks + group * CG + cl * V;
   // an equal share of the block's contiguous nonzero range per unit
   const uint32_t len = (E - A + NU - 1) / NU;
   const uint32_t u0 = min(E, A + unit * len), u1 = min(E, u0 + len);
@@ -631,17 +634,20 @@ __global__ void __launch_bounds__(kThreads, 3)
   // CG lanes of this slot (uniform trip count across the warp)
   int cell = 0;
   const unsigned slot_bits =
-      (CG == 32 ? 0xffffffffu : ((1u << CG) - 1u)) << (slot * CG);
-  for (int base = 0; base < nxc; base += CG)
+      (LS == 32 ? 0xffffffffu : ((1u << LS) - 1u)) << (slot * LS);
+  for (int base = 0; base < nxc; base += LS)
   {
-    const int i = base + coil + 1;
+    const int i = base + cl + 1;
     const bool le = i <= nxc && s_off[i] <= u0;
     cell += __popc(__ballot_sync(0xffffffffu, le) & slot_bits);
   }
   if (u0 < u1)
   {
     uint32_t bound = s_off[cell + 1];
-    float ax = 0.f, ay = 0.f;
+    float ax[V], ay[V];
+#pragma unroll
+    for (int v = 0; v < V; ++v)
+      ax[v] = ay[v] = 0.f;
     // a cell boundary: the finished cell lies inside this share (store) or
     // started in an earlier share (head partial)
 #define GN_SPMM_FLUSH(KK)                                                      \
@@ -649,16 +655,31 @@ __global__ void __launch_bounds__(kThreads, 3)
   {                                                                            \
     if (s_off[cell] < u0)                                                      \
     {                                                                          \
-      part_head[unit][coil] = make_float2(ax, ay);                             \
-      if (coil == 0)                                                           \
+      _Pragma("unroll") for (int v = 0; v < V; ++v)                            \
+          part_head[unit][cl * V + v] = make_float2(ax[v], ay[v]);             \
+      if (cl == 0)                                                             \
         head_cell[unit] = cell;                                                \
     }                                                                          \
     else                                                                       \
-      acc_s[cell][coil] = make_float2(ax, ay);                                 \
-    ax = ay = 0.f;                                                             \
+    {                                                                          \
+      _Pragma("unroll") for (int v = 0; v < V; ++v)                            \
+          acc_s[cell][cl * V + v] = make_float2(ax[v], ay[v]);                 \
+    }                                                                          \
+    _Pragma("unroll") for (int v = 0; v < V; ++v) ax[v] = ay[v] = 0.f;        \
     ++cell;                                                                    \
     bound = s_off[cell + 1];                                                   \
   }
+  // k-space values of a lane's V coils for sample row q
+#define GN_SPMM_LOAD(DST, Q)                                                   \
+  if (V == 2)                                                                  \
+  {                                                                            \
+    const float4 f4 = __ldg(reinterpret_cast<const float4 *>(                  \
+        ksg + (Q) * (uint32_t)CP));                                            \
+    DST[0] = make_float2(f4.x, f4.y);                                          \
+    DST[V - 1] = make_float2(f4.z, f4.w);                                      \
+  }                                                                            \
+  else                                                                         \
+    DST[0] = __ldg(ksg + (Q) * (uint32_t)CP);
     // whole batches of B entries: the next batch's (sample, weight) pairs
     // load while this batch's k-space rows are read
     const uint32_t kfull = u0 + (u1 - u0) / B * B;
@@ -671,10 +692,12 @@ __global__ void __launch_bounds__(kThreads, 3)
         q[u] = __ldg(nz + k0 + u);
       for (; k0 < kfull; k0 += B)
       {
-        float2 v[B];
+        float2 vv[B][V];
 #pragma unroll
         for (int u = 0; u < B; ++u)
-          v[u] = __ldg(ksg + q[u].x * (uint32_t)CP);
+        {
+          GN_SPMM_LOAD(vv[u], q[u].x)
+        }
         uint2 qn[B];
 #pragma unroll
         for (int u = 0; u < B; ++u)
@@ -687,8 +710,12 @@ __global__ void __launch_bounds__(kThreads, 3)
         {
           GN_SPMM_FLUSH(k0 + u)
           const float w = __uint_as_float(q[u].y);
-          ax = __fmaf_rn(w, v[u].x, ax);
-          ay = __fmaf_rn(w, v[u].y, ay);
+#pragma unroll
+          for (int v = 0; v < V; ++v)
+          {
+            ax[v] = __fmaf_rn(w, vv[u][v].x, ax[v]);
+            ay[v] = __fmaf_rn(w, vv[u][v].y, ay[v]);
+          }
         }
 #pragma unroll
         for (int u = 0; u < B; ++u)
@@ -698,25 +725,39 @@ __global__ void __launch_bounds__(kThreads, 3)
     for (; k0 < u1; ++k0)
     {  // the remainder, one entry at a time
       const uint2 q = __ldg(nz + k0);
-      const float2 v = __ldg(ksg + q.x * (uint32_t)CP);
+      float2 vv[V];
+      GN_SPMM_LOAD(vv, q.x)
       GN_SPMM_FLUSH(k0)
       const float w = __uint_as_float(q.y);
-      ax = __fmaf_rn(w, v.x, ax);
-      ay = __fmaf_rn(w, v.y, ay);
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+      {
+        ax[v] = __fmaf_rn(w, vv[v].x, ax[v]);
+        ay[v] = __fmaf_rn(w, vv[v].y, ay[v]);
+      }
     }
+#undef GN_SPMM_LOAD
 #undef GN_SPMM_FLUSH
     if (s_off[cell] < u0)
     {
-      part_head[unit][coil] = make_float2(ax, ay);
-      if (coil == 0)
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        part_head[unit][cl * V + v] = make_float2(ax[v], ay[v]);
+      if (cl == 0)
         head_cell[unit] = cell;
     }
     else if (bound <= u1)
-      acc_s[cell][coil] = make_float2(ax, ay);
+    {
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        acc_s[cell][cl * V + v] = make_float2(ax[v], ay[v]);
+    }
     else
     {
-      part_tail[unit][coil] = make_float2(ax, ay);
-      if (coil == 0)
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        part_tail[unit][cl * V + v] = make_float2(ax[v], ay[v]);
+      if (cl == 0)
         tail_cell[unit] = cell;
     }
   }
@@ -725,13 +766,18 @@ __global__ void __launch_bounds__(kThreads, 3)
     const int tc = tail_cell[unit];
     if (tc >= 0)
     {
-      float2 sum = part_tail[unit][coil];
-      for (int v = unit + 1; v < NU && head_cell[v] == tc; ++v)
+#pragma unroll
+      for (int v = 0; v < V; ++v)
       {
-        sum.x = __fadd_rn(sum.x, part_head[v][coil].x);
-        sum.y = __fadd_rn(sum.y, part_head[v][coil].y);
+        const int c = cl * V + v;
+        float2 sum = part_tail[unit][c];
+        for (int u = unit + 1; u < NU && head_cell[u] == tc; ++u)
+        {
+          sum.x = __fadd_rn(sum.x, part_head[u][c].x);
+          sum.y = __fadd_rn(sum.y, part_head[u][c].y);
+        }
+        acc_s[tc][c] = sum;
       }
-      acc_s[tc][coil] = sum;
     }
   }
   __syncthreads();
@@ -1520,17 +1566,17 @@ void launch_adjoint_spmm(const uint32_t *row_off, const uint2 *nz,
   const int cg = spmm_coil_group(C);
   dim3 grd(g.G[1] * g.G[2], (g.G[0] + kSpmmCells - 1) / kSpmmCells,
            (C + cg - 1) / cg);
-#define GN_SPMM(CGV)                                                           \
-  k_adjoint_spmm<CGV><<<grd, kThreads, 0, s>>>(row_off, nz, ks, CP, g, C,     \
-                                               shift ? 1 : 0, grid)
+#define GN_SPMM(CGV, VV)                                                       \
+  k_adjoint_spmm<CGV, VV><<<grd, kThreads, 0, s>>>(row_off, nz, ks, CP, g, C, \
+                                                   shift ? 1 : 0, grid)
   switch (cg)
   {
-  case 1: GN_SPMM(1); break;
-  case 2: GN_SPMM(2); break;
-  case 4: GN_SPMM(4); break;
-  case 8: GN_SPMM(8); break;
-  case 16: GN_SPMM(16); break;
-  default: GN_SPMM(32); break;
+  case 1: GN_SPMM(1, 1); break;
+  case 2: GN_SPMM(2, 1); break;
+  case 4: GN_SPMM(4, 1); break;
+  case 8: GN_SPMM(8, 1); break;
+  case 16: GN_SPMM(16, 1); break;
+  default: GN_SPMM(32, 2); break;
   }
 #undef GN_SPMM
   GN_LAUNCH_CHECK("adjoint spmm");
