@@ -1064,17 +1064,20 @@ __global__ void __launch_bounds__(kThreads)
             "l"(tm), "r"(x0), "r"(base[1]), "r"(c0), "r"(bar)
             : "memory");
     }
-    __syncthreads();
-    uint32_t done = 0;
-    for (long long i = 0; i < kMbarSpin && !done; ++i)
-      asm volatile(
-          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], "
-          "0; selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(bar)
-          : "memory");
-    if (!done)
-      s_fail = 1;
+    if (threadIdx.x == 0)
+    {  // one thread waits (bounded); the others wait at the barrier below,
+       // which orders the copied tile before their reads
+      uint32_t done = 0;
+      for (long long i = 0; i < kMbarSpin && !done; ++i)
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
+            "[%1], 0; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+      if (!done)
+        s_fail = 1;
+    }
     __syncthreads();
     if (s_fail)
     {  // the copy did not complete: report, do not use the tile

@@ -42,7 +42,7 @@ thread_local std::string g_last_error;
 
 // Candidates per adjoint work item and samples per forward work item.
 constexpr int kAdjPayload = 2048;
-constexpr int kFwdPayload = 1024;
+constexpr int kFwdPayload = 512;
 
 // Mirrors the upstream IndPair (gpuNUFFT_types.hpp:33-49): compared by the
 // second member only, so libstdc++'s std::sort produces the upstream order.
@@ -304,10 +304,8 @@ void build_items(gnufft_plan &p)
       fitems.push_back(
           FwdItem{s, (int)k, (int)std::min<uint32_t>(e, k + kFwdPayload), 0});
   }
-  std::stable_sort(fitems.begin(), fitems.end(),
-                   [](const FwdItem &a, const FwdItem &b) {
-                     return (a.end - a.begin) > (b.end - b.begin);
-                   });
+  // sector order: consecutive blocks take neighbouring tiles, whose halos
+  // overlap, so much of a tile comes from L2
   p.n_fwd_items = (int)fitems.size();
   upload(p.fwd_items, fitems.data(), fitems.size(), p.stream);
 }
