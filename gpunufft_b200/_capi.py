@@ -43,7 +43,7 @@ EXPORTED = (
     "gnufft_forward_device", "gnufft_set_timing", "gnufft_get_stage_times",
     "gnufft_last_error", "gnufft_status_string", "gnufft_version",
     "gnufft_adjoint_convolution_noalloc",
-    "gnufft_traj_grad_device",
+    "gnufft_traj_grad_device", "gnufft_set_sens_device",
 )
 
 
@@ -120,6 +120,8 @@ def lib() -> ctypes.CDLL:
     L.gnufft_export_tables.argtypes = [_P] + [_P] * 8
     L.gnufft_set_sens.restype = st
     L.gnufft_set_sens.argtypes = [_P, _P, _U]
+    L.gnufft_set_sens_device.restype = st
+    L.gnufft_set_sens_device.argtypes = [_P, _P, _U, _P]
     for name in ("gnufft_adjoint_host", "gnufft_forward_host"):
         f = getattr(L, name)
         f.restype = st

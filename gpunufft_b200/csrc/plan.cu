@@ -976,6 +976,30 @@ gnufft_status gnufft_set_sens(gnufft_plan *p, const void *sens,
   });
 }
 
+gnufft_status gnufft_set_sens_device(gnufft_plan *p, const void *sens,
+                                     uint32_t n_coils, void *stream)
+{
+  if (!p)
+    return (gnufft_status)fail(kInvalidArgument, "plan is NULL");
+  if (!sens || n_coils == 0)
+    return (gnufft_status)fail(kInvalidArgument, "no maps given");
+  if (p->plain)
+    return (gnufft_status)fail(kNotSupported,
+                               "plain plans take host maps (gnufft_set_sens)");
+  return guarded([&] {
+    DeviceGuard dg(p->desc.device);
+    const size_t n = (size_t)n_coils * p->g.img_count;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // the copy is ordered on `stream` only: work on other streams that may
+    // still read the previous maps must be ordered before it by the caller
+    p->sens.ensure(n * sizeof(float2));
+    GN_CUDA(cudaMemcpyAsync(p->sens.get(), sens, n * sizeof(float2),
+                            cudaMemcpyDeviceToDevice, s));
+    p->sens_h.clear();
+    p->sens_coils = n_coils;
+  });
+}
+
 gnufft_status gnufft_set_timing(gnufft_plan *p, int enable)
 {
   if (!p)

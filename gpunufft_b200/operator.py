@@ -203,6 +203,18 @@ class Plan:
                             int(f["operator_type"]), device=device)
 
     def set_sens(self, sens) -> None:
+        """Replace the maps (host arrays; CUDA tensors are copied on the
+        device, ordered on the current torch stream)."""
+        if _is_cuda_tensor(sens):
+            t = sens.reshape(-1).to(torch.complex64).contiguous()
+            n = t.numel() // self.n_img
+            if n * self.n_img != t.numel():
+                raise ValueError("sensitivity maps do not match the image")
+            stream = torch.cuda.current_stream(t.device).cuda_stream
+            C.check(C.lib().gnufft_set_sens_device(
+                self._h, t.data_ptr(), n, ctypes.c_void_p(stream)))
+            self.n_sens = n
+            return
         if sens is None:
             C.check(C.lib().gnufft_set_sens(self._h, None, 0))
             self.n_sens = 0

@@ -86,18 +86,27 @@ def estimate_bytes(req: Request) -> int:
 
 
 class PlanCache:
-    """Operators resident per trajectory.  Several instances of one
-    trajectory's operator exist only while several requests use it at the
-    same time; idle instances stay cached until memory is needed."""
+    """Operators resident per trajectory (sector tables, interpolation
+    matrix, transform plans and scratch).  At most ``max_instances``
+    instances of one trajectory's operator exist; a request whose
+    trajectory's instances are all busy waits for one (building another
+    costs more than most requests' whole solve).  Idle instances stay cached
+    until memory is needed."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, max_instances: int = 1):
         self.device = device
+        self.max_instances = max_instances
         self.free: Dict[str, List[Plan]] = collections.defaultdict(list)
         self.busy: Dict[int, str] = {}
+        self.count: Dict[str, int] = collections.defaultdict(int)
         self.lru: "collections.OrderedDict[str, float]" = \
             collections.OrderedDict()
         self.hits = 0
         self.misses = 0
+
+    def available(self, req: Request) -> bool:
+        key = _key(req)
+        return bool(self.free[key]) or self.count[key] < self.max_instances
 
     def acquire(self, req: Request) -> Plan:
         key = _key(req)
@@ -111,6 +120,7 @@ class PlanCache:
             p = Plan(req.traj, req.img_dims, req.kernel_width,
                      req.sector_width, req.osf, req.dens, None, C.BALANCED,
                      device=self.device)
+            self.count[key] += 1
         self.busy[id(p)] = key
         return p
 
@@ -127,6 +137,7 @@ class PlanCache:
         for key in list(self.lru):
             if self.free.get(key):
                 self.free[key].pop().close()
+                self.count[key] -= 1
                 if not self.free[key] and key not in self.busy.values():
                     del self.lru[key]
                 return True
@@ -137,6 +148,7 @@ class PlanCache:
             for p in ps:
                 p.close()
         self.free.clear()
+        self.count.clear()
 
 
 class _Active:
@@ -150,9 +162,10 @@ class _Active:
         self.it = 0
         with torch.cuda.stream(self.stream):
             dev = torch.device("cuda", device)
-            self.y = torch.from_numpy(np.ascontiguousarray(
-                req.kspace, np.complex64)).to(dev, non_blocking=True)
-            plan.set_sens(req.sens)
+            # pinned host tensors upload asynchronously on this stream
+            self.y = torch.as_tensor(req.kspace).to(dev, non_blocking=True)
+            self.maps = torch.as_tensor(req.sens).to(dev, non_blocking=True)
+            plan.set_sens(self.maps)
             rhs = plan.adjoint(self.y)
             self.x = torch.zeros_like(rhs)
             self.r = rhs
@@ -219,20 +232,29 @@ class Server:
         self.queue.append(req)
 
     def _admit(self) -> None:
+        """Admit queued requests in arrival order while slots and memory
+        allow; a request whose trajectory's operator is busy stays queued
+        without blocking the requests behind it."""
+        waiting = collections.deque()
         while self.queue and len(self.active) < self.max_slots:
-            req = self.queue[0]
+            req = self.queue.popleft()
+            if not self.cache.available(req):
+                waiting.append(req)
+                continue
             need = estimate_bytes(req)
             while (self.in_use + need + self.cache.idle_bytes() > self.budget
                    and self.cache.evict_one()):
                 pass
             if self.in_use + need > self.budget:
-                break                       # wait for memory to free up
-            self.queue.popleft()
+                waiting.append(req)         # wait for memory to free up
+                break
             req.admitted = self.now()
             plan = self.cache.acquire(req)
             self.active.append(_Active(req, plan, self.device))
             self.in_use += need
             self.peak_in_use = max(self.peak_in_use, self.in_use)
+        waiting.extend(self.queue)
+        self.queue = waiting
         self.max_concurrent = max(self.max_concurrent, len(self.active))
 
     def _retire(self) -> None:
@@ -263,6 +285,8 @@ class Server:
         serve until all are done.  Returns the finished requests."""
         pending = collections.deque(sorted(arrivals, key=lambda r: r.arrival))
         self._t0 = time.perf_counter()
+        self.done = []
+        self.max_concurrent = 0
         n = len(pending)
         while len(self.done) < n:
             t = self.now()

@@ -185,6 +185,15 @@ GNUFFT_API gnufft_status gnufft_export_tables(const gnufft_plan *plan, float *tr
 GNUFFT_API gnufft_status gnufft_set_sens(gnufft_plan *plan, const void *sens,
                               uint32_t n_coils);
 
+/* Replace the sensitivity maps from DEVICE memory: complex64
+ * [n_coils][image] copied device-to-device into the plan, ordered on
+ * `stream` (no host copy, no synchronisation; for serving loops that keep
+ * maps on the GPU).  Not for plans created with GNUFFT_FLAG_PLAIN, which
+ * stream host maps per coil like the upstream. */
+GNUFFT_API gnufft_status gnufft_set_sens_device(gnufft_plan *plan,
+                                       const void *sens, uint32_t n_coils,
+                                       void *stream);
+
 /* Adjoint NUFFT.  kspace: complex64 [n_coils][M]; image (output):
  *   CONVOLUTION / DENSITY_ESTIMATION: raw grid [n_coils][grid]
  *   FFT: [n_coils][image] after inverse FFT, crop and 1/sqrt(grid count)
