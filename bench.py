@@ -386,9 +386,12 @@ def run_gpu_arm(args, rank, world, dist):
     # (8 B per sample per coil), coordinates (4 B per axis per sample) and
     # the oversampled grid (8 B per cell per coil)
     gbytes = 8 * M * C + 4 * dim * M + 8 * G_cells * C
+    # the forward interpolation of the pruned-transform path (power-of-two
+    # grids, this workload) is k_forward_tma; k_forward_interp otherwise
+    fwd_kernel = "k_forward_tma" if all(
+        (v & (v - 1)) == 0 for v in g.grid_dims if v) else "k_forward_interp"
     kernels = {
-        "k_forward_interp": ("forward interpolation", avg("fwd",
-                                                          "gridding_ms")),
+        fwd_kernel: ("forward interpolation", avg("fwd", "gridding_ms")),
         "k_adjoint_spmm": ("adjoint gridding", avg("adj", "gridding_ms")),
     }
     rooflines = []
