@@ -37,7 +37,7 @@ template <int L> struct Shape
   static size_t smem() { return (size_t)(L + NL * R1 * YP) * sizeof(float2); }
   // column passes: TC adjacent columns per block, so that every warp moves
   // 32 * 8 bytes (L <= 256) of one row per access
-  static constexpr int TC = L <= 256 ? 32 : (L == 512 ? 16 : 8);
+  static constexpr int TC = L <= 256 ? 16 : (L == 512 ? 16 : 8);
   static constexpr int CT = TC * T;            // threads per column block
   static size_t col_smem()
   {
