@@ -511,4 +511,40 @@ size_t build_interp_matrix(const float *traj_sorted,
   return n;
 }
 
+
+namespace
+{
+// Range of z (grid cells with at least one interpolation weight) per (y, x)
+// column, widened by one cell each way; empty columns keep lo > hi.
+__global__ void k_col_ranges(const uint32_t *__restrict__ row_off, int G0,
+                             int G1, int G2, uint2 *__restrict__ range)
+{
+  const long long n = (long long)G0 * G1 * G2;
+  for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x)
+  {
+    if (row_off[c + 1] == row_off[c])
+      continue;
+    const long long col = c % ((long long)G0 * G1);
+    const int z = (int)(c / ((long long)G0 * G1));
+    atomicMin(&range[col].x, (unsigned)max(z - 1, 0));
+    atomicMax(&range[col].y, (unsigned)min(z + 1, G2 - 1));
+  }
+}
+}  // namespace
+
+void build_column_ranges(const uint32_t *row_off, const Geo &g,
+                         DeviceBuffer &range, cudaStream_t s)
+{
+  const size_t cols = (size_t)g.G[0] * g.G[1];
+  range.reset(cols * sizeof(uint2));
+  std::vector<uint2> init(cols, make_uint2(0xFFFFFFFFu, 0u));
+  GN_CUDA(cudaMemcpyAsync(range.get(), init.data(), cols * sizeof(uint2),
+                          cudaMemcpyHostToDevice, s));
+  k_col_ranges<<<grid_for(g.grid_count, 256, 148 * 64), 256, 0, s>>>(
+      row_off, g.G[0], g.G[1], g.G[2], range.as<uint2>());
+  GN_LAUNCH_CHECK("column ranges");
+  GN_CUDA(cudaStreamSynchronize(s));
+}
+
 }  // namespace gnufft

@@ -61,4 +61,10 @@ size_t build_interp_matrix(const float *traj_sorted,
                            DeviceBuffer &row_off, DeviceBuffer &nz,
                            cudaStream_t s);
 
+// Per (y, x) column of the grid, the range [lo, hi] of z cells that carry
+// interpolation weights (widened by one; lo > hi when none): the forward
+// transform writes only these cells, the only ones the interpolation reads.
+void build_column_ranges(const uint32_t *row_off, const Geo &g,
+                         DeviceBuffer &range, cudaStream_t s);
+
 }  // namespace gnufft

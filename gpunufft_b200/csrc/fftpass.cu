@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(Shape<L>::CT)
     k_fft_cols(const float2 *__restrict__ src, float2 *__restrict__ dst,
                long long ncols, int src_rows, int dst_rows, int in_add,
                int in_count, int out_add, int out_count,
-               const float2 *__restrict__ roots)
+               const float2 *__restrict__ roots,
+               const uint2 *__restrict__ colrange)
 {
   using S = Shape<L>;
   extern __shared__ float2 sm[];
@@ -197,7 +198,11 @@ __global__ void __launch_bounds__(Shape<L>::CT)
   const int cl = threadIdx.x % S::TC, lt = threadIdx.x / S::TC;
   const long long col = (long long)blockIdx.x * S::TC + cl;
   const long long plane = blockIdx.y;
-  const bool on = col < ncols;
+  // optional output row range of the column (rows outside are not needed)
+  uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
+  if (colrange && col < ncols)
+    cr = __ldg(colrange + col);
+  const bool on = col < ncols && cr.x <= cr.y;
   // exchange slots of the block's columns interleaved: slot * TC + column
   float2 *Y = Ybase + cl;
   const float2 *sp = src + plane * src_rows * ncols + col;
@@ -228,7 +233,7 @@ __global__ void __launch_bounds__(Shape<L>::CT)
       for (int k2 = 0; k2 < S::R2; ++k2)
       {
         const int r = (lt + S::R1 * k2 + out_add) & (L - 1);
-        if (r < out_count)
+        if (r < out_count && (unsigned)r >= cr.x && (unsigned)r <= cr.y)
           dp[(long long)r * ncols] = b[k2];
       }
     }
@@ -511,7 +516,7 @@ template <bool INV>
 void cols(int L, const float2 *src, float2 *dst, long long ncols,
           int src_rows, int dst_rows, long long planes, int in_add,
           int in_count, int out_add, int out_count, const float2 *roots,
-          cudaStream_t s)
+          cudaStream_t s, const uint2 *colrange = nullptr)
 {
   with_length(L, [&](auto lc) {
     constexpr int LL = decltype(lc)::value;
@@ -524,7 +529,7 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
                     (unsigned)planes);
     k<<<grid, S::CT, S::col_smem(), s>>>(src, dst, ncols, src_rows,
                                           dst_rows, in_add, in_count, out_add,
-                                          out_count, roots);
+                                          out_count, roots, colrange);
     GN_LAUNCH_CHECK("pruned column transform");
   });
 }
@@ -566,7 +571,8 @@ size_t pruned_scratch_b(const Geo &g, int C)
 void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
-                           float2 *tmp_b, float2 *grid, cudaStream_t s)
+                           float2 *tmp_b, float2 *grid, cudaStream_t s,
+                           const uint2 *zrange)
 {
   const long long N = g.img_count;
   const long long rows = (long long)g.N[1] * g.N[2];
@@ -608,7 +614,7 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                 g.G[2], C,
                 pos_mod((long long)g.shift_inv[2] - g.crop[2], g.G[2]),
                 g.N[2], pos_mod(-(long long)g.shift_fwd[2], g.G[2]), g.G[2],
-                roots[2], s);
+                roots[2], s, zrange);
 }
 
 void launch_pruned_adjoint(const float2 *grid, const float *deapo,

@@ -43,10 +43,13 @@ size_t pruned_scratch_b(const Geo &g, int C);
 // -> FORWARD fftshift -> grid [C][G] (so cell q of the shifted spectrum, the
 // one the interpolation reads, is stored at q).
 // roots[a]: the root table of axis a (length G[a]).
+// zrange (3-D, optional): per (y, x) column the z rows to write; the
+// others are left as they are (the interpolation never reads them).
 void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
-                           float2 *tmp_b, float2 *grid, cudaStream_t s);
+                           float2 *tmp_b, float2 *grid, cudaStream_t s,
+                           const uint2 *zrange = nullptr);
 
 // Adjoint: grid [C][G] (INVERSE fftshift folded in by the adjoint spread)
 // -> unnormalised inverse DFT -> crop of the second INVERSE fftshift ->

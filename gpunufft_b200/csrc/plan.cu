@@ -88,6 +88,7 @@ struct gnufft_plan
   DeviceBuffer w_rows, w_nz;  // interpolation matrix, CSR by grid cell
   DeviceBuffer dlut;          // kernel derivative table (trajectory gradient)
   DeviceBuffer roots[3];      // DFT roots per axis (pruned transforms)
+  DeviceBuffer zrange;        // per (y, x) column: z rows with weights
   float dlut_mult = 0.f;
   size_t nnz = 0;
   int n_adj_items = 0, n_split = 0, n_fwd_items = 0;
@@ -135,7 +136,7 @@ struct gnufft_plan
                                   &ks,          &grid,        &stage_in,
                                   &stage_out,   &one_sens,    &fft_a,
                                   &fft_b,       &dlut,        &roots[0],
-                                  &roots[1],    &roots[2]};
+                                  &roots[1],    &roots[2],    &zrange};
     size_t s = 0;
     for (auto *b : bufs)
       s += b->bytes();
@@ -378,6 +379,8 @@ void finish_tables(gnufft_plan &p)
                               p.sec_sorted.as<uint32_t>(), p.M, p.g,
                               p.lut.as<float>(), p.w_rows, p.w_nz, p.stream);
   build_items(p);
+  if (p.pruned && p.dim == 3)
+    build_column_ranges(p.w_rows.as<uint32_t>(), p.g, p.zrange, p.stream);
   processing_order(p.sdc_h, p.order_h);
   upload(p.deapo, p.deapo_h.data(), p.deapo_h.size(), p.stream);
   GN_CUDA(cudaStreamSynchronize(p.stream));
@@ -659,7 +662,8 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
     p.mark(4, s);
     launch_pruned_forward(img, sens, p.deapo.as<float>(), g, (int)C,
                           root_ptrs(p).data(), p.fft_a.as<float2>(),
-                          p.fft_b.as<float2>(), grid, s);
+                          p.fft_b.as<float2>(), grid, s,
+                          p.zrange.as<uint2>());
     p.launches += g.dim;
     p.mark(5, s);
     p.mark(2, s);
