@@ -12,169 +12,13 @@
 #include <type_traits>
 
 #include "devutil.hpp"
+#include "fftcore.cuh"
 
 namespace gnufft
 {
 namespace
 {
-constexpr int kFftThreads = 256;
-
-template <int L> struct Split;
-template <> struct Split<16> { static constexpr int R1 = 4, R2 = 4; };
-template <> struct Split<32> { static constexpr int R1 = 8, R2 = 4; };
-template <> struct Split<64> { static constexpr int R1 = 8, R2 = 8; };
-template <> struct Split<128> { static constexpr int R1 = 16, R2 = 8; };
-template <> struct Split<256> { static constexpr int R1 = 16, R2 = 16; };
-template <> struct Split<512> { static constexpr int R1 = 32, R2 = 16; };
-template <> struct Split<1024> { static constexpr int R1 = 32, R2 = 32; };
-
-template <int L> struct Shape
-{
-  static constexpr int R1 = Split<L>::R1, R2 = Split<L>::R2;
-  static constexpr int T = R1 > R2 ? R1 : R2;  // threads per line
-  static constexpr int NL = kFftThreads / T;   // lines per block (rows)
-  static constexpr int YP = R2 + 1;            // padded exchange row
-  static size_t smem() { return (size_t)(L + NL * R1 * YP) * sizeof(float2); }
-  // column passes: TC adjacent columns per block, so that every warp moves
-  // 32 * 8 bytes (L <= 256) of one row per access
-  static constexpr int TC = L <= 256 ? 16 : (L == 512 ? 16 : 8);
-  static constexpr int CT = TC * T;            // threads per column block
-  static size_t col_smem()
-  {
-    return (size_t)(L + TC * R1 * YP) * sizeof(float2);
-  }
-};
-
-__host__ __device__ constexpr int bitrev(int i, int R)
-{
-  int r = 0;
-  for (int b = 1; b < R; b <<= 1)
-  {
-    r = (r << 1) | (i & 1);
-    i >>= 1;
-  }
-  return r;
-}
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b)
-{
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-__host__ __device__ constexpr int ilog2(int v)
-{
-  int r = 0;
-  while ((1 << r) < v)
-    ++r;
-  return r;
-}
-
-// In-register radix-2 DIT DFT of R points, natural order in and out.
-// w[k] = exp(-2 pi i k / RM), k < RM / 2, RM >= R (conjugated for the
-// inverse).  Every loop has a constant trip count and every index is a
-// constant, so data and roots stay in registers.
-template <int R, int RM, bool INV>
-__device__ __forceinline__ void reg_fft(float2 (&a)[R],
-                                        const float2 (&w)[RM / 2])
-{
-#pragma unroll
-  for (int i = 0; i < R; ++i)
-  {
-    const int j = bitrev(i, R);
-    if (j > i)
-    {
-      const float2 t = a[i];
-      a[i] = a[j];
-      a[j] = t;
-    }
-  }
-  constexpr int LOG = ilog2(R);
-#pragma unroll
-  for (int st = 0; st < LOG; ++st)
-  {
-    const int half = 1 << st;
-#pragma unroll
-    for (int b = 0; b < R / 2; ++b)
-    {
-      const int k = b & (half - 1);
-      const int i0 = ((b >> st) << (st + 1)) + k;
-      const int i1 = i0 + half;
-      const float2 u = a[i0];
-      float2 v = a[i1];
-      if (k != 0)
-      {
-        float2 r = w[k * (RM >> (st + 1))];
-        if (INV)
-          r.y = -r.y;
-        v = cmul(v, r);
-      }
-      a[i0] = make_float2(u.x + v.x, u.y + v.y);
-      a[i1] = make_float2(u.x - v.x, u.y - v.y);
-    }
-  }
-}
-
-// Stage 1 of a line (thread lt < R2 holds a[j] = x[lt + R2 j]): R1-point
-// DFT, twiddle, store to the line's exchange slots Y[(k1 * YP + lt) * YS]
-// (YS: stride between consecutive slots of one line, so that lines can be
-// interleaved for conflict-free access).
-template <int L> struct Rm
-{
-  static constexpr int V = Shape<L>::T;  // roots kept for the larger DFT
-};
-
-template <int L, bool INV, int YS>
-__device__ __forceinline__ void stage1(float2 (&a)[Shape<L>::R1], int lt,
-                                       const float2 (&w)[Rm<L>::V / 2],
-                                       const float2 *__restrict__ tw,
-                                       float2 *__restrict__ Y)
-{
-  using S = Shape<L>;
-  reg_fft<S::R1, Rm<L>::V, INV>(a, w);
-#pragma unroll
-  for (int k1 = 0; k1 < S::R1; ++k1)
-  {
-    float2 v = a[k1];
-    if (k1 != 0)
-    {
-      float2 r = tw[(lt * k1) & (L - 1)];
-      if (INV)
-        r.y = -r.y;
-      v = cmul(v, r);
-    }
-    Y[(k1 * S::YP + lt) * YS] = v;
-  }
-}
-
-// Stage 2 (thread lt < R1): b[k2] = X[lt + R1 k2].
-template <int L, bool INV, int YS>
-__device__ __forceinline__ void stage2(float2 (&b)[Shape<L>::R2], int lt,
-                                       const float2 (&w)[Rm<L>::V / 2],
-                                       const float2 *__restrict__ Y)
-{
-  using S = Shape<L>;
-#pragma unroll
-  for (int t = 0; t < S::R2; ++t)
-    b[t] = Y[(lt * S::YP + t) * YS];
-  reg_fft<S::R2, Rm<L>::V, INV>(b, w);
-}
-
-template <int L>
-__device__ __forceinline__ void load_reg_roots(float2 (&w)[Rm<L>::V / 2],
-                                               const float2 *tw)
-{
-  constexpr int RM = Rm<L>::V;
-#pragma unroll
-  for (int k = 0; k < RM / 2; ++k)
-    w[k] = tw[k * (L / RM)];
-}
-
-__device__ __forceinline__ void load_roots(float2 *tw, const float2 *roots,
-                                           int L)
-{
-  for (int i = threadIdx.x; i < L; i += blockDim.x)
-    tw[i] = __ldg(roots + i);
-}
+using namespace fftcore;
 
 // --------------------------------------------------------------------------
 // column passes: lines along a strided axis, columns contiguous
@@ -237,6 +81,137 @@ __global__ void __launch_bounds__(Shape<L>::CT)
           dp[(long long)r * ncols] = b[k2];
       }
     }
+  }
+}
+
+// --------------------------------------------------------------------------
+// last adjoint pass along a strided axis, fused with the image stages
+// --------------------------------------------------------------------------
+// Columns contiguous (TC per block); each block runs every coil of its
+// columns in turn: inverse DFT, crop + shift (output k holds image index
+// (k + out_add) mod L when < n_out), 1/sqrt(Ng), deapodization and the
+// conj(S) coil sum in coil order (or per-coil outputs).  src: coil c,
+// row r, column col at c * coil_stride + r * ncols + col; image pixel of
+// output row n and column col: n * ncols + col.
+template <int L, bool SENS>
+__global__ void __launch_bounds__(Shape<L>::CT)
+    k_fft_cols_sum(const float2 *__restrict__ src, long long ncols,
+                   long long coil_stride, const float *__restrict__ deapo,
+                   const float2 *__restrict__ sens, int n_out, long long N,
+                   int C, int coils_per_block, int out_add, float scale,
+                   int stage, int accumulate,
+                   const float2 *__restrict__ roots, float2 *__restrict__ out,
+                   float2 *__restrict__ partial)
+{
+  using S = Shape<L>;
+  extern __shared__ float2 sm[];
+  float2 *tw = sm;
+  float2 *Ybase = sm + L;
+  load_roots(tw, roots, L);
+  const int cl = threadIdx.x % S::TC, lt = threadIdx.x / S::TC;
+  const long long col = (long long)blockIdx.x * S::TC + cl;
+  const bool on = col < ncols;
+  float2 *Y = Ybase + cl;
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  float2 acc[S::R2];
+#pragma unroll
+  for (int k2 = 0; k2 < S::R2; ++k2)
+    acc[k2] = make_float2(0.f, 0.f);
+  const int c0 = blockIdx.y * coils_per_block;
+  const int c1 = min(C, c0 + coils_per_block);
+  for (int c = c0; c < c1; ++c)
+  {
+    if (lt < S::R2)
+    {
+      const float2 *sp = src + (long long)c * coil_stride + col;
+      float2 a[S::R1];
+#pragma unroll
+      for (int j = 0; j < S::R1; ++j)
+        a[j] = on ? __ldg(sp + (long long)(lt + S::R2 * j) * ncols)
+                  : make_float2(0.f, 0.f);
+      stage1<L, true, S::TC>(a, lt, w, tw, Y);
+    }
+    __syncthreads();
+    if (lt < S::R1 && on)
+    {
+      float2 b[S::R2];
+      stage2<L, true, S::TC>(b, lt, w, Y);
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int n = (lt + S::R1 * k2 + out_add) & (L - 1);
+        if (n >= n_out)
+          continue;
+        const long long px = (long long)n * ncols + col;
+        // crop -> FFT scaling -> deapodization (gpuNUFFT_operator.cpp:
+        // 800-819)
+        float2 v = make_float2(__fmul_rn(b[k2].x, scale),
+                               __fmul_rn(b[k2].y, scale));
+        if (stage == 2)
+        {
+          const float d = __ldg(deapo + px);
+          v.x = __fmul_rn(v.x, d);
+          v.y = __fmul_rn(v.y, d);
+        }
+        if (SENS && stage == 2)
+        {  // conj(S) * v, running coil sum (std_gpuNUFFT_kernels.cu:158-218)
+          const float2 sv = __ldg(sens + c * N + px);
+          acc[k2].x += v.x * sv.x + v.y * sv.y;
+          acc[k2].y += v.y * sv.x - v.x * sv.y;
+        }
+        else
+          out[c * N + px] = v;
+      }
+    }
+    __syncthreads();
+  }
+  if (SENS && stage == 2 && lt < S::R1 && on)
+  {
+#pragma unroll
+    for (int k2 = 0; k2 < S::R2; ++k2)
+    {
+      const int n = (lt + S::R1 * k2 + out_add) & (L - 1);
+      if (n >= n_out)
+        continue;
+      const long long px = (long long)n * ncols + col;
+      if (partial)
+      {  // one coil group of several: summed in group order afterwards
+        partial[blockIdx.y * N + px] = acc[k2];
+        continue;
+      }
+      float2 r = acc[k2];
+      if (accumulate)
+      {
+        const float2 o = out[px];
+        r = make_float2(o.x + r.x, o.y + r.y);
+      }
+      out[px] = r;
+    }
+  }
+}
+
+__global__ void k_sum_coil_groups(const float2 *__restrict__ partial,
+                                  int groups, long long N, int accumulate,
+                                  float2 *__restrict__ out)
+{
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < N;
+       p += (long long)gridDim.x * blockDim.x)
+  {
+    float2 r = make_float2(0.f, 0.f);
+    for (int k = 0; k < groups; ++k)
+    {
+      const float2 v = partial[k * N + p];
+      r.x += v.x;
+      r.y += v.y;
+    }
+    if (accumulate)
+    {
+      const float2 o = out[p];
+      r = make_float2(o.x + r.x, o.y + r.y);
+    }
+    out[p] = r;
   }
 }
 
@@ -669,6 +644,80 @@ void launch_pruned_adjoint(const float2 *grid, const float *deapo,
     }
     GN_LAUNCH_CHECK("pruned adjoint rows");
   });
+}
+
+
+void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
+                                  const float2 *sens, const Geo &g, int C,
+                                  int stage, int accumulate,
+                                  const float2 *const roots[3],
+                                  float2 *tmp_b, float2 *part, float2 *out,
+                                  cudaStream_t s)
+{
+  const long long N = g.img_count;
+  const float2 *src = xrows;
+  long long ncols = g.N[0];
+  int ax = 1;  // the axis of the last pass
+  if (g.dim == 3)
+  {  // y: [C][G_z][G_y][N_x] -> [C][G_z][N_y][N_x]
+    cols<true>(g.G[1], xrows, tmp_b, g.N[0], g.G[1], g.N[1],
+               (long long)C * g.G[2], 0, g.G[1],
+               pos_mod(-(long long)g.crop[1] - g.shift_inv[1], g.G[1]),
+               g.N[1], roots[1], s);
+    src = tmp_b;
+    ncols = (long long)g.N[1] * g.N[0];
+    ax = 2;
+  }
+  const long long coil_stride = (long long)g.G[ax] * ncols;
+  const int out_add =
+      pos_mod(-(long long)g.crop[ax] - g.shift_inv[ax], g.G[ax]);
+  with_length(g.G[ax], [&](auto lc) {
+    constexpr int LL = decltype(lc)::value;
+    using S = Shape<LL>;
+    const long long nb = (ncols + S::TC - 1) / S::TC;
+    // coil groups in separate blocks when the columns alone do not fill
+    // the GPU (eight blocks per SM); their coil sums meet in `partial`
+    int groups = 1;
+    while (groups < C && nb * groups < 148LL * 8)
+      groups *= 2;
+    if (groups > C)
+      groups = C;
+    const int cpb = (C + groups - 1) / groups;
+    groups = (C + cpb - 1) / cpb;
+    const bool combine = sens != nullptr && stage == 2;
+    float2 *partial = (combine && groups > 1) ? part : nullptr;
+    const dim3 grd((unsigned)nb, (unsigned)groups);
+    if (combine)
+    {
+      auto k = k_fft_cols_sum<LL, true>;
+      set_smem(k, S::col_smem());
+      k<<<grd, S::CT, S::col_smem(), s>>>(src, ncols, coil_stride, deapo,
+                                         sens, g.N[ax], N, C, cpb, out_add,
+                                         g.fft_scale, stage, accumulate,
+                                         roots[ax], out, partial);
+    }
+    else
+    {
+      auto k = k_fft_cols_sum<LL, false>;
+      set_smem(k, S::col_smem());
+      k<<<grd, S::CT, S::col_smem(), s>>>(src, ncols, coil_stride, deapo,
+                                         nullptr, g.N[ax], N, C, cpb, out_add,
+                                         g.fft_scale, stage, accumulate,
+                                         roots[ax], out, nullptr);
+    }
+    GN_LAUNCH_CHECK("pruned adjoint last pass");
+    if (partial)
+    {
+      k_sum_coil_groups<<<grid_for(N, 256, 148 * 16), 256, 0, s>>>(
+          partial, groups, N, accumulate, out);
+      GN_LAUNCH_CHECK("coil-group sum");
+    }
+  });
+}
+
+size_t pruned_scratch_xfirst(const Geo &g, int C)
+{
+  return g.dim == 3 ? (size_t)C * g.G[2] * g.N[1] * g.N[0] : 0;
 }
 
 }  // namespace gnufft

@@ -62,4 +62,17 @@ void launch_pruned_adjoint(const float2 *grid, const float *deapo,
                            float2 *tmp_a, float2 *tmp_b, float2 *out,
                            cudaStream_t s);
 
+// The adjoint with the x transform done first (fused into the spread,
+// launch_adjoint_spmm_xfft): xrows [C][G_z][G_y][N_x] -> (3-D) y pass into
+// tmp_b [C][G_z][N_y][N_x] -> last pass (z in 3-D, y in 2-D) fused with
+// crop, 1/sqrt(Ng), deapodization and the conj(S) coil sum (per coil group,
+// the groups' sums added in group order through `part`, C x N complex).
+void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
+                                  const float2 *sens, const Geo &g, int C,
+                                  int stage, int accumulate,
+                                  const float2 *const roots[3],
+                                  float2 *tmp_b, float2 *part, float2 *out,
+                                  cudaStream_t s);
+size_t pruned_scratch_xfirst(const Geo &g, int C);
+
 }  // namespace gnufft

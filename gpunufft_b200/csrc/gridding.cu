@@ -20,10 +20,12 @@
 #include "gridding.cuh"
 
 #include <algorithm>
+#include <type_traits>
 
 #include <cuda.h>
 
 #include "devutil.hpp"
+#include "fftcore.cuh"
 #include "footprint.cuh"
 
 namespace gnufft
@@ -566,63 +568,23 @@ __global__ void k_zero_targets(const int *__restrict__ targets, Geo g, int C,
 // (INVERSE fftshift folded into the store position).
 constexpr int kSpmmCells = 64;
 
-// V coils per lane (V = 2 reads a lane's two coils as one 16-byte load and
-// halves the per-entry instructions per coil).
+// The streaming accumulation of a block's cell range [0, nxc) (offsets
+// s_off, nonzeros from s_off[0] to s_off[nxc]) for the CG coils of `group`:
+// equal shares of the nonzeros per warp slot, running cell sums in
+// registers, cells cut by share boundaries finished in slot order.  acc
+// (pitch CG + 1) must be zero and head/tail_cell -1 on entry (after a
+// barrier); acc holds every cell after the caller's next barrier.
 template <int CG, int V>
-__global__ void __launch_bounds__(kThreads, 3)
-    k_adjoint_spmm(const uint32_t *__restrict__ row_off,
-                   const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
-                   int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
+__device__ __forceinline__ void spmm_accumulate(
+    const uint32_t *s_off, int nxc, const uint2 *__restrict__ nz,
+    const float2 *__restrict__ ks, int CP, int group, float2 *acc,
+    float2 *part_head, float2 *part_tail, int *head_cell, int *tail_cell)
 {
   constexpr int LS = CG / V;          // lanes per slot
   constexpr int SLOTS = 32 / LS;
   constexpr int NU = kWarps * SLOTS;  // streaming units per block
   constexpr int B = 8 / V;            // entries per batch
-  __shared__ float2 acc_s[kSpmmCells][CG + 1];
-  __shared__ uint32_t s_off[kSpmmCells + 1];
-  // partial sums of cells cut by share boundaries: head = the unit's first
-  // cell when it started in an earlier share, tail = its last cell when it
-  // started in this share and continues in the next
-  __shared__ float2 part_head[NU][CG], part_tail[NU][CG];
-  __shared__ int head_cell[NU], tail_cell[NU];
-  const int x0 = blockIdx.y * kSpmmCells;
-  const int row = blockIdx.x;  // y + G1 * z
-  const int group = blockIdx.z;
-  const int nxc = min(kSpmmCells, g.G[0] - x0);
-  const long long rowbase = (long long)row * g.G[0] + x0;
-  for (int i = threadIdx.x; i <= nxc; i += kThreads)
-    s_off[i] = __ldg(row_off + rowbase + i);
-  __syncthreads();
   const uint32_t A = s_off[0], E = s_off[nxc];
-  // output row after the optional INVERSE fftshift
-  int y = row % g.G[1], z = row / g.G[1];
-  if (shift)
-  {
-    y = wrap_mod(y - g.shift_inv[1], g.G[1]);
-    z = wrap_mod(z - g.shift_inv[2], g.G[2]);
-  }
-  const long long orow = ((long long)z * g.G[1] + y) * g.G[0];
-  if (A == E)
-  {  // no sample reaches these cells: plain zero stores
-    for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
-    {
-      const int cl = idx / kSpmmCells, xi = idx - cl * kSpmmCells;
-      const int c = group * CG + cl;
-      if (xi >= nxc || c >= C)
-        continue;
-      int x = x0 + xi;
-      if (shift)
-        x = wrap_mod(x - g.shift_inv[0], g.G[0]);
-      grid[(long long)c * g.grid_count + orow + x] = make_float2(0.f, 0.f);
-    }
-    return;
-  }
-  for (int i = threadIdx.x; i < kSpmmCells * (CG + 1); i += kThreads)
-    (&acc_s[0][0])[i] = make_float2(0.f, 0.f);
-  for (int i = threadIdx.x; i < NU; i += kThreads)
-    head_cell[i] = tail_cell[i] = -1;
-  __syncthreads();
-
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int slot = lane / LS, cl = lane % LS;
   const int unit = warp * SLOTS + slot;
@@ -656,14 +618,14 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (s_off[cell] < u0)                                                      \
     {                                                                          \
       _Pragma("unroll") for (int v = 0; v < V; ++v)                            \
-          part_head[unit][cl * V + v] = make_float2(ax[v], ay[v]);             \
+          part_head[unit * CG + cl * V + v] = make_float2(ax[v], ay[v]);             \
       if (cl == 0)                                                             \
         head_cell[unit] = cell;                                                \
     }                                                                          \
     else                                                                       \
     {                                                                          \
       _Pragma("unroll") for (int v = 0; v < V; ++v)                            \
-          acc_s[cell][cl * V + v] = make_float2(ax[v], ay[v]);                 \
+          acc[cell * (CG + 1) + cl * V + v] = make_float2(ax[v], ay[v]);                 \
     }                                                                          \
     _Pragma("unroll") for (int v = 0; v < V; ++v) ax[v] = ay[v] = 0.f;        \
     ++cell;                                                                    \
@@ -742,7 +704,7 @@ __global__ void __launch_bounds__(kThreads, 3)
     {
 #pragma unroll
       for (int v = 0; v < V; ++v)
-        part_head[unit][cl * V + v] = make_float2(ax[v], ay[v]);
+        part_head[unit * CG + cl * V + v] = make_float2(ax[v], ay[v]);
       if (cl == 0)
         head_cell[unit] = cell;
     }
@@ -750,13 +712,13 @@ __global__ void __launch_bounds__(kThreads, 3)
     {
 #pragma unroll
       for (int v = 0; v < V; ++v)
-        acc_s[cell][cl * V + v] = make_float2(ax[v], ay[v]);
+        acc[cell * (CG + 1) + cl * V + v] = make_float2(ax[v], ay[v]);
     }
     else
     {
 #pragma unroll
       for (int v = 0; v < V; ++v)
-        part_tail[unit][cl * V + v] = make_float2(ax[v], ay[v]);
+        part_tail[unit * CG + cl * V + v] = make_float2(ax[v], ay[v]);
       if (cl == 0)
         tail_cell[unit] = cell;
     }
@@ -770,16 +732,75 @@ __global__ void __launch_bounds__(kThreads, 3)
       for (int v = 0; v < V; ++v)
       {
         const int c = cl * V + v;
-        float2 sum = part_tail[unit][c];
+        float2 sum = part_tail[unit * CG + c];
         for (int u = unit + 1; u < NU && head_cell[u] == tc; ++u)
         {
-          sum.x = __fadd_rn(sum.x, part_head[u][c].x);
-          sum.y = __fadd_rn(sum.y, part_head[u][c].y);
+          sum.x = __fadd_rn(sum.x, part_head[u * CG + c].x);
+          sum.y = __fadd_rn(sum.y, part_head[u * CG + c].y);
         }
-        acc_s[tc][c] = sum;
+        acc[tc * (CG + 1) + c] = sum;
       }
     }
   }
+}
+
+// V coils per lane (V = 2 reads a lane's two coils as one 16-byte load and
+// halves the per-entry instructions per coil).
+template <int CG, int V>
+__global__ void __launch_bounds__(kThreads, 3)
+    k_adjoint_spmm(const uint32_t *__restrict__ row_off,
+                   const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
+                   int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
+{
+  constexpr int NU = kWarps * (32 / (CG / V));  // streaming units
+  __shared__ float2 acc_s[kSpmmCells][CG + 1];
+  __shared__ uint32_t s_off[kSpmmCells + 1];
+  // partial sums of cells cut by share boundaries: head = the unit's first
+  // cell when it started in an earlier share, tail = its last cell when it
+  // started in this share and continues in the next
+  __shared__ float2 part_head[NU][CG], part_tail[NU][CG];
+  __shared__ int head_cell[NU], tail_cell[NU];
+  const int x0 = blockIdx.y * kSpmmCells;
+  const int row = blockIdx.x;  // y + G1 * z
+  const int group = blockIdx.z;
+  const int nxc = min(kSpmmCells, g.G[0] - x0);
+  const long long rowbase = (long long)row * g.G[0] + x0;
+  for (int i = threadIdx.x; i <= nxc; i += kThreads)
+    s_off[i] = __ldg(row_off + rowbase + i);
+  __syncthreads();
+  const uint32_t A = s_off[0], E = s_off[nxc];
+  // output row after the optional INVERSE fftshift
+  int y = row % g.G[1], z = row / g.G[1];
+  if (shift)
+  {
+    y = wrap_mod(y - g.shift_inv[1], g.G[1]);
+    z = wrap_mod(z - g.shift_inv[2], g.G[2]);
+  }
+  const long long orow = ((long long)z * g.G[1] + y) * g.G[0];
+  if (A == E)
+  {  // no sample reaches these cells: plain zero stores
+    for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
+    {
+      const int cl = idx / kSpmmCells, xi = idx - cl * kSpmmCells;
+      const int c = group * CG + cl;
+      if (xi >= nxc || c >= C)
+        continue;
+      int x = x0 + xi;
+      if (shift)
+        x = wrap_mod(x - g.shift_inv[0], g.G[0]);
+      grid[(long long)c * g.grid_count + orow + x] = make_float2(0.f, 0.f);
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < kSpmmCells * (CG + 1); i += kThreads)
+    (&acc_s[0][0])[i] = make_float2(0.f, 0.f);
+  for (int i = threadIdx.x; i < NU; i += kThreads)
+    head_cell[i] = tail_cell[i] = -1;
+  __syncthreads();
+
+  spmm_accumulate<CG, V>(s_off, nxc, nz, ks, CP, group, &acc_s[0][0],
+                         &part_head[0][0], &part_tail[0][0], head_cell,
+                         tail_cell);
   __syncthreads();
   for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
   {
@@ -791,6 +812,111 @@ __global__ void __launch_bounds__(kThreads, 3)
     if (shift)
       x = wrap_mod(x - g.shift_inv[0], g.G[0]);
     grid[(long long)c * g.grid_count + orow + x] = acc_s[xi][cl];
+  }
+}
+
+// --------------------------------------------------------------------------
+// adjoint spread of whole grid rows with the inverse x transform fused
+// --------------------------------------------------------------------------
+// One block per (grid row (z, y), coil group): the row's G_x cells are
+// accumulated like k_adjoint_spmm (deterministic, no atomics) into shared
+// memory, then each coil's row is transformed along x (inverse DFT, INVERSE
+// fftshift of the grid folded into the input index) and only the N_x cropped
+// outputs are written: out [C][G_z][G_y][N_x] (rows in the INVERSE-shifted
+// frame the next passes expect).  The grid itself is never written.
+// Shared memory: acc [L][CG + 1] | roots [L] | exchange area, which first
+// holds the spread's offsets and partial sums.
+template <int CG, int V, int L>
+__global__ void __launch_bounds__(kThreads)
+    k_adjoint_spmm_xfft(const uint32_t *__restrict__ row_off,
+                        const uint2 *__restrict__ nz,
+                        const float2 *__restrict__ ks, int CP, Geo g, int C,
+                        const float2 *__restrict__ roots,
+                        float2 *__restrict__ out)
+{
+  using S = fftcore::Shape<L>;
+  static_assert(S::T * S::NL == kThreads, "one line per T threads");
+  constexpr int NU = kWarps * (32 / (CG / V));
+  extern __shared__ __align__(16) unsigned char smraw[];
+  float2 *acc = reinterpret_cast<float2 *>(smraw);
+  float2 *tw = acc + L * (CG + 1);
+  float2 *ex = tw + L;  // exchange area
+  float2 *part_head = ex;
+  float2 *part_tail = part_head + NU * CG;
+  uint32_t *s_off = reinterpret_cast<uint32_t *>(part_tail + NU * CG);
+  int *head_cell = reinterpret_cast<int *>(s_off + L + 1);
+  int *tail_cell = head_cell + NU;
+  const int row = blockIdx.x;  // y + G1 * z
+  const int group = blockIdx.y;
+  const int y = wrap_mod(row % g.G[1] - g.shift_inv[1], g.G[1]);
+  const int z = wrap_mod(row / g.G[1] - g.shift_inv[2], g.G[2]);
+  const long long rowbase = (long long)row * L;
+  for (int i = threadIdx.x; i <= L; i += kThreads)
+    s_off[i] = __ldg(row_off + rowbase + i);
+  fftcore::load_roots(tw, roots, L);
+  __syncthreads();
+  const bool empty = s_off[0] == s_off[L];
+  const int Nx = g.N[0];
+  const long long plane = (long long)g.G[2] * g.G[1] * Nx;
+  const long long orow = ((long long)z * g.G[1] + y) * Nx;
+  if (empty)
+  {  // no sample reaches this row: its transform is zero
+    for (int i = threadIdx.x; i < CG * Nx; i += kThreads)
+    {
+      const int cl = i / Nx, x = i - cl * Nx;
+      const int c = group * CG + cl;
+      if (c < C)
+        out[(long long)c * plane + orow + x] = make_float2(0.f, 0.f);
+    }
+    return;
+  }
+  for (int i = threadIdx.x; i < L * (CG + 1); i += kThreads)
+    acc[i] = make_float2(0.f, 0.f);
+  for (int i = threadIdx.x; i < NU; i += kThreads)
+    head_cell[i] = tail_cell[i] = -1;
+  __syncthreads();
+  spmm_accumulate<CG, V>(s_off, L, nz, ks, CP, group, acc, part_head,
+                         part_tail, head_cell, tail_cell);
+  __syncthreads();
+
+  // inverse DFT along x of each coil's row, NL coils per pass
+  float2 w[fftcore::Rm<L>::V / 2];
+  fftcore::load_reg_roots<L>(w, tw);
+  const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
+  float2 *Y = ex + line * S::R1 * S::YP;
+  // FFT input n holds the cell stored at n: logical x = (n + floor(G/2))
+  const int sx = g.shift_inv[0];
+  // FFT output k holds image x = (k - crop - floor(G/2)) mod G when < N
+  int out_add = (-(g.crop[0] + g.shift_inv[0])) % L;
+  if (out_add < 0)
+    out_add += L;
+  for (int cb = 0; cb < CG; cb += S::NL)
+  {
+    const int cl = cb + line;
+    if (lt < S::R2 && cl < CG)
+    {
+      float2 a[S::R1];
+#pragma unroll
+      for (int j = 0; j < S::R1; ++j)
+        a[j] = acc[((lt + S::R2 * j + sx) & (L - 1)) * (CG + 1) + cl];
+      fftcore::stage1<L, true, 1>(a, lt, w, tw, Y);
+    }
+    __syncthreads();
+    const int c = group * CG + cl;
+    if (lt < S::R1 && cl < CG && c < C)
+    {
+      float2 b[S::R2];
+      fftcore::stage2<L, true, 1>(b, lt, w, Y);
+      float2 *o = out + (long long)c * plane + orow;
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int x = (lt + S::R1 * k2 + out_add) & (L - 1);
+        if (x < Nx)
+          o[x] = b[k2];
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -1786,6 +1912,82 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
 #undef GN_TMA_KS
 #undef GN_TMA
   GN_LAUNCH_CHECK("forward interpolation (tensor-copy tiles)");
+  return true;
+}
+
+
+int spmm_xfft_coils(int L)
+{
+  // accumulation rows of L x (coils + 1) complex values stay near 64 KB
+  return L <= 256 ? 32 : (L == 512 ? 16 : 8);
+}
+
+bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
+                              const float2 *ks, int CP, const Geo &g, int C,
+                              const float2 *roots_x, float2 *out,
+                              cudaStream_t s)
+{
+  const int L = g.G[0];
+  if (L < 16 || L > 1024 || (L & (L - 1)))
+    return false;
+  const int cgmax = spmm_xfft_coils(L);
+  // the spread's coil group must divide the k-space lane count CP
+  int cg = spmm_coil_group(C);
+  if (cg > cgmax)
+    cg = cgmax;
+  if (CP % cg)
+    return false;
+  const int v = cg == 32 ? 2 : 1;
+  const dim3 grd((unsigned)((long long)g.G[1] * g.G[2]),
+                 (unsigned)((C + cg - 1) / cg));
+  bool ok = true;
+  auto go = [&](auto lc, auto cgc, auto vc) {
+    constexpr int LL = decltype(lc)::value;
+    constexpr int CGV = decltype(cgc)::value;
+    constexpr int VV = decltype(vc)::value;
+    using S = fftcore::Shape<LL>;
+    constexpr int NU = kWarps * (32 / (CGV / VV));
+    const size_t head = (size_t)(LL * (CGV + 1) + LL) * sizeof(float2);
+    const size_t spread = (size_t)2 * NU * CGV * sizeof(float2) +
+                          (size_t)(LL + 1) * 4 + (size_t)2 * NU * 4;
+    const size_t exch = (size_t)S::NL * S::R1 * S::YP * sizeof(float2);
+    const size_t smem = head + (spread > exch ? spread : exch);
+    if (smem > 220 * 1024)
+    {
+      ok = false;
+      return;
+    }
+    auto k = k_adjoint_spmm_xfft<CGV, VV, LL>;
+    GN_CUDA(cudaFuncSetAttribute(
+        k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grd, kThreads, smem, s>>>(row_off, nz, ks, CP, g, C, roots_x, out);
+  };
+  using I = std::integral_constant<int, 1>;
+  using I2 = std::integral_constant<int, 2>;
+  auto with_cg = [&](auto lc) {
+    switch (cg)
+    {
+    case 1: go(lc, std::integral_constant<int, 1>(), I()); break;
+    case 2: go(lc, std::integral_constant<int, 2>(), I()); break;
+    case 4: go(lc, std::integral_constant<int, 4>(), I()); break;
+    case 8: go(lc, std::integral_constant<int, 8>(), I()); break;
+    case 16: go(lc, std::integral_constant<int, 16>(), I()); break;
+    default: go(lc, std::integral_constant<int, 32>(), I2()); break;
+    }
+  };
+  switch (L)
+  {
+  case 16: with_cg(std::integral_constant<int, 16>()); break;
+  case 32: with_cg(std::integral_constant<int, 32>()); break;
+  case 64: with_cg(std::integral_constant<int, 64>()); break;
+  case 128: with_cg(std::integral_constant<int, 128>()); break;
+  case 256: with_cg(std::integral_constant<int, 256>()); break;
+  case 512: with_cg(std::integral_constant<int, 512>()); break;
+  default: with_cg(std::integral_constant<int, 1024>()); break;
+  }
+  if (!ok)
+    return false;
+  GN_LAUNCH_CHECK("adjoint spread with x transform");
   return true;
 }
 

@@ -73,6 +73,15 @@ void launch_adjoint_spmm(const uint32_t *row_off, const uint2 *nz,
                          const float2 *ks, int CP, const Geo &g, int C,
                          bool shift, float2 *grid, cudaStream_t s);
 
+// Adjoint spread of whole grid rows with the inverse DFT along x fused:
+// out [C][G_z][G_y][N_x] (the cropped x outputs of every INVERSE-shifted
+// grid row; the grid itself is not written).  Returns false (nothing
+// launched) when the row length or coil grouping does not suit it.
+bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
+                              const float2 *ks, int CP, const Geo &g, int C,
+                              const float2 *roots_x, float2 *out,
+                              cudaStream_t s);
+
 // Adjoint finish: crop of the (shifted) inverse-FFT output, 1/sqrt(Ng),
 // deapodization, conj(sens) multiply and coil sum.  stage: 1 = FFT (crop +
 // scale per coil), 2 = DEAPODIZATION.  With `accumulate` (maps only) the

@@ -558,7 +558,9 @@ void ensure_pruned(gnufft_plan &p, uint32_t C, cudaStream_t s)
       GN_CUDA(cudaStreamSynchronize(s));
     }
   p.fft_a.ensure(pruned_scratch_a(p.g, (int)C) * sizeof(float2));
-  p.fft_b.ensure(pruned_scratch_b(p.g, (int)C) * sizeof(float2));
+  p.fft_b.ensure(std::max(pruned_scratch_b(p.g, (int)C),
+                          pruned_scratch_xfirst(p.g, (int)C)) *
+                 sizeof(float2));
 }
 
 std::array<const float2 *, 3> root_ptrs(const gnufft_plan &p)
@@ -593,6 +595,29 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
   p.launches += 1;
   p.mark(1, s);
   p.mark(2, s);
+  if (p.pruned && !conv)
+  {  // spread whole grid rows with the inverse x transform fused (the grid
+     // buffer receives only the cropped x outputs), then y and z
+    ensure_pruned(p, C, s);
+    if (launch_adjoint_spmm_xfft(p.w_rows.as<uint32_t>(), p.w_nz.as<uint2>(),
+                                 p.ks.as<float2>(), CP, g, (int)C,
+                                 p.roots[0].as<float2>(), grid, s))
+    {
+      p.launches += 1;
+      p.mark(3, s);
+      p.mark(4, s);
+      launch_pruned_adjoint_xfirst(
+          grid, p.deapo.as<float>(),
+          stage == GNUFFT_DEAPODIZATION ? sens : nullptr, g, (int)C,
+          stage == GNUFFT_FFT ? 1 : 2, accumulate, root_ptrs(p).data(),
+          p.fft_b.as<float2>(), p.fft_a.as<float2>(), img, s);
+      p.launches += g.dim - 1;
+      p.mark(5, s);
+      p.mark(6, s);
+      p.mark(7, s);
+      return;
+    }
+  }
   launch_adjoint_spmm(p.w_rows.as<uint32_t>(), p.w_nz.as<uint2>(),
                       p.ks.as<float2>(), CP, g, (int)C, !conv, grid, s);
   p.launches += 1;
