@@ -97,7 +97,11 @@ __device__ __forceinline__ void reg_fft(float2 (&a)[R],
       const int i1 = i0 + half;
       const float2 u = a[i0];
       float2 v = a[i1];
-      if (k != 0)
+      if (2 * k == half)
+      {  // the quarter-turn root -i (+i inverse): exact, no multiply
+        v = INV ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+      }
+      else if (k != 0)
       {
         float2 r = w[k * (RM >> (st + 1))];
         if (INV)

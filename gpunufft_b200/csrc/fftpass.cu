@@ -94,7 +94,7 @@ __global__ void __launch_bounds__(Shape<L>::CT)
 // row r, column col at c * coil_stride + r * ncols + col; image pixel of
 // output row n and column col: n * ncols + col.
 template <int L, bool SENS>
-__global__ void __launch_bounds__(Shape<L>::CT)
+__global__ void __launch_bounds__(Shape<L>::CT, L <= 256 ? 3 : 1)
     k_fft_cols_sum(const float2 *__restrict__ src, long long ncols,
                    long long coil_stride, const float *__restrict__ deapo,
                    const float2 *__restrict__ sens, int n_out, long long N,
