@@ -568,17 +568,39 @@ __global__ void k_zero_targets(const int *__restrict__ targets, Geo g, int C,
 // (INVERSE fftshift folded into the store position).
 constexpr int kSpmmCells = 64;
 
+// Position of (cell, coil c) in a spread accumulator of CG coils per cell:
+// rows padded to CG + 1 (SR2 == 0), or rows of CG with the coil index
+// XOR-swizzled by the cell (SR2 = R2 of the row transform that runs in place
+// on the accumulator).  The swizzle flips coil bits 1-3 only, so coil pairs
+// stay adjacent (16-byte stores), and it varies with both cell % SR2 and
+// cell / SR2, so that the transform's stage-1 accesses (cells r0 + lt) and
+// stage-2 accesses (cells k1 * SR2 + t) each spread over all banks.
+template <int CG, int SR2>
+__device__ __forceinline__ int acc_pos(int cell, int c)
+{
+  if constexpr (SR2 == 0)
+    return cell * (CG + 1) + c;
+  else
+  {
+    const int sw = ((cell % SR2) ^ (cell / SR2)) & 7;
+    return cell * CG + (c ^ (sw << 1));
+  }
+}
+
 // The streaming accumulation of a block's cell range [0, nxc) (offsets
 // s_off, nonzeros from s_off[0] to s_off[nxc]) for the CG coils of `group`:
 // equal shares of the nonzeros per warp slot, running cell sums in
 // registers, cells cut by share boundaries finished in slot order.  acc
-// (pitch CG + 1) must be zero and head/tail_cell -1 on entry (after a
-// barrier); acc holds every cell after the caller's next barrier.
-template <int CG, int V>
+// (laid out by acc_pos<CG, SR2>) must be zero and head/tail_cell -1 on
+// entry (after a barrier); acc holds every cell after the caller's next
+// barrier.  A unit whose last cell continues in the next shares leaves its
+// partial sum in acc; the following units' partials (part_head) are added
+// to it in unit order.
+template <int CG, int V, int SR2 = 0>
 __device__ __forceinline__ void spmm_accumulate(
     const uint32_t *s_off, int nxc, const uint2 *__restrict__ nz,
     const float2 *__restrict__ ks, int CP, int group, float2 *acc,
-    float2 *part_head, float2 *part_tail, int *head_cell, int *tail_cell)
+    float2 *part_head, int *head_cell, int *tail_cell)
 {
   constexpr int LS = CG / V;          // lanes per slot
   constexpr int SLOTS = 32 / LS;
@@ -625,7 +647,7 @@ __device__ __forceinline__ void spmm_accumulate(
     else                                                                       \
     {                                                                          \
       _Pragma("unroll") for (int v = 0; v < V; ++v)                            \
-          acc[cell * (CG + 1) + cl * V + v] = make_float2(ax[v], ay[v]);                 \
+          acc[acc_pos<CG, SR2>(cell, cl * V + v)] = make_float2(ax[v], ay[v]);  \
     }                                                                          \
     _Pragma("unroll") for (int v = 0; v < V; ++v) ax[v] = ay[v] = 0.f;        \
     ++cell;                                                                    \
@@ -708,18 +730,13 @@ __device__ __forceinline__ void spmm_accumulate(
       if (cl == 0)
         head_cell[unit] = cell;
     }
-    else if (bound <= u1)
-    {
-#pragma unroll
-      for (int v = 0; v < V; ++v)
-        acc[cell * (CG + 1) + cl * V + v] = make_float2(ax[v], ay[v]);
-    }
     else
-    {
+    {  // the cell started in this share; if it continues in the next
+       // shares, this is its first partial sum
 #pragma unroll
       for (int v = 0; v < V; ++v)
-        part_tail[unit * CG + cl * V + v] = make_float2(ax[v], ay[v]);
-      if (cl == 0)
+        acc[acc_pos<CG, SR2>(cell, cl * V + v)] = make_float2(ax[v], ay[v]);
+      if (bound > u1 && cl == 0)
         tail_cell[unit] = cell;
     }
   }
@@ -732,13 +749,14 @@ __device__ __forceinline__ void spmm_accumulate(
       for (int v = 0; v < V; ++v)
       {
         const int c = cl * V + v;
-        float2 sum = part_tail[unit * CG + c];
+        const int pos = acc_pos<CG, SR2>(tc, c);
+        float2 sum = acc[pos];
         for (int u = unit + 1; u < NU && head_cell[u] == tc; ++u)
         {
           sum.x = __fadd_rn(sum.x, part_head[u * CG + c].x);
           sum.y = __fadd_rn(sum.y, part_head[u * CG + c].y);
         }
-        acc[tc * (CG + 1) + c] = sum;
+        acc[pos] = sum;
       }
     }
   }
@@ -755,10 +773,10 @@ __global__ void __launch_bounds__(kThreads, 3)
   constexpr int NU = kWarps * (32 / (CG / V));  // streaming units
   __shared__ float2 acc_s[kSpmmCells][CG + 1];
   __shared__ uint32_t s_off[kSpmmCells + 1];
-  // partial sums of cells cut by share boundaries: head = the unit's first
-  // cell when it started in an earlier share, tail = its last cell when it
-  // started in this share and continues in the next
-  __shared__ float2 part_head[NU][CG], part_tail[NU][CG];
+  // cells cut by share boundaries: head = the partial sum of the unit's
+  // first cell when it started in an earlier share, tail = its last cell
+  // when it started in this share and continues in the next
+  __shared__ float2 part_head[NU][CG];
   __shared__ int head_cell[NU], tail_cell[NU];
   const int x0 = blockIdx.y * kSpmmCells;
   const int row = blockIdx.x;  // y + G1 * z
@@ -799,7 +817,7 @@ __global__ void __launch_bounds__(kThreads, 3)
   __syncthreads();
 
   spmm_accumulate<CG, V>(s_off, nxc, nz, ks, CP, group, &acc_s[0][0],
-                         &part_head[0][0], &part_tail[0][0], head_cell,
+                         &part_head[0][0], head_cell,
                          tail_cell);
   __syncthreads();
   for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
@@ -824,10 +842,41 @@ __global__ void __launch_bounds__(kThreads, 3)
 // fftshift of the grid folded into the input index) and only the N_x cropped
 // outputs are written: out [C][G_z][G_y][N_x] (rows in the INVERSE-shifted
 // frame the next passes expect).  The grid itself is never written.
-// Shared memory: acc [L][CG + 1] | roots [L] | exchange area, which first
-// holds the spread's offsets and partial sums.
+// With 32 coils per group (L <= 256) the row transforms run in place on the
+// accumulator (coil-swizzled rows, acc_pos), which keeps the block near
+// 72 KB at L = 256 (three blocks per SM).  Shared memory: acc | roots [L] |
+// spread scratch (partial sums, offsets), followed, for the other coil
+// groups (acc rows padded to CG + 1), by an exchange area for the
+// transform that overlaps the scratch.
+// accumulation rows of L x coils complex values stay near 64 KB
+constexpr int xfft_max_coils(int L)
+{
+  return L <= 256 ? 32 : (L == 512 ? 16 : 8);
+}
+
+template <int CG, int L> struct XfftLayout
+{
+  using S = fftcore::Shape<L>;
+  static constexpr bool IP = CG == 32 && L <= 256;
+  static constexpr int SR2 = IP ? S::R2 : 0;
+  static constexpr int ACC = IP ? L * CG : L * (CG + 1);
+  static size_t scratch(int NU)
+  {
+    return (size_t)NU * CG * sizeof(float2) + (size_t)(L + 1) * 4 +
+           (size_t)2 * NU * 4;
+  }
+  static size_t smem(int NU)
+  {
+    const size_t head = (size_t)(ACC + L) * sizeof(float2);
+    const size_t exch =
+        IP ? 0 : (size_t)S::NL * S::R1 * S::YP * sizeof(float2);
+    const size_t sc = scratch(NU);
+    return head + (sc > exch ? sc : exch);
+  }
+};
+
 template <int CG, int V, int L>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, L <= 256 ? 3 : 1)
     k_adjoint_spmm_xfft(const uint32_t *__restrict__ row_off,
                         const uint2 *__restrict__ nz,
                         const float2 *__restrict__ ks, int CP, Geo g, int C,
@@ -835,15 +884,18 @@ __global__ void __launch_bounds__(kThreads)
                         float2 *__restrict__ out)
 {
   using S = fftcore::Shape<L>;
+  using Lay = XfftLayout<CG, L>;
+  constexpr bool IP = Lay::IP;
+  constexpr int SR2 = Lay::SR2;
   static_assert(S::T * S::NL == kThreads, "one line per T threads");
+  static_assert(S::T <= 32, "a line's threads share a warp");
   constexpr int NU = kWarps * (32 / (CG / V));
-  extern __shared__ __align__(16) unsigned char smraw[];
+  extern __shared__ __align__(128) unsigned char smraw[];
   float2 *acc = reinterpret_cast<float2 *>(smraw);
-  float2 *tw = acc + L * (CG + 1);
-  float2 *ex = tw + L;  // exchange area
+  float2 *tw = acc + Lay::ACC;
+  float2 *ex = tw + L;  // scratch, then (padded layout) exchange area
   float2 *part_head = ex;
-  float2 *part_tail = part_head + NU * CG;
-  uint32_t *s_off = reinterpret_cast<uint32_t *>(part_tail + NU * CG);
+  uint32_t *s_off = reinterpret_cast<uint32_t *>(part_head + NU * CG);
   int *head_cell = reinterpret_cast<int *>(s_off + L + 1);
   int *tail_cell = head_cell + NU;
   const int row = blockIdx.x;  // y + G1 * z
@@ -870,53 +922,102 @@ __global__ void __launch_bounds__(kThreads)
     }
     return;
   }
-  for (int i = threadIdx.x; i < L * (CG + 1); i += kThreads)
-    acc[i] = make_float2(0.f, 0.f);
+  {
+    float4 *a4 = reinterpret_cast<float4 *>(acc);
+    for (int i = threadIdx.x; i < Lay::ACC / 2; i += kThreads)
+      a4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  }
   for (int i = threadIdx.x; i < NU; i += kThreads)
     head_cell[i] = tail_cell[i] = -1;
   __syncthreads();
-  spmm_accumulate<CG, V>(s_off, L, nz, ks, CP, group, acc, part_head,
-                         part_tail, head_cell, tail_cell);
+  spmm_accumulate<CG, V, SR2>(s_off, L, nz, ks, CP, group, acc, part_head,
+                              head_cell, tail_cell);
   __syncthreads();
 
   // inverse DFT along x of each coil's row, NL coils per pass
   float2 w[fftcore::Rm<L>::V / 2];
   fftcore::load_reg_roots<L>(w, tw);
   const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
-  float2 *Y = ex + line * S::R1 * S::YP;
   // FFT input n holds the cell stored at n: logical x = (n + floor(G/2))
   const int sx = g.shift_inv[0];
   // FFT output k holds image x = (k - crop - floor(G/2)) mod G when < N
   int out_add = (-(g.crop[0] + g.shift_inv[0])) % L;
   if (out_add < 0)
     out_add += L;
+  // writes the N_x cropped outputs of a transformed line
+  auto store = [&](const float2(&b)[S::R2], int c) {
+    float2 *o = out + (long long)c * plane + orow;
+#pragma unroll
+    for (int k2 = 0; k2 < S::R2; ++k2)
+    {
+      const int x = (lt + S::R1 * k2 + out_add) & (L - 1);
+      if (x < Nx)
+        o[x] = b[k2];
+    }
+  };
   for (int cb = 0; cb < CG; cb += S::NL)
   {
     const int cl = cb + line;
-    if (lt < S::R2 && cl < CG)
-    {
-      float2 a[S::R1];
-#pragma unroll
-      for (int j = 0; j < S::R1; ++j)
-        a[j] = acc[((lt + S::R2 * j + sx) & (L - 1)) * (CG + 1) + cl];
-      fftcore::stage1<L, true, 1>(a, lt, w, tw, Y);
-    }
-    __syncthreads();
     const int c = group * CG + cl;
-    if (lt < S::R1 && cl < CG && c < C)
-    {
-      float2 b[S::R2];
-      fftcore::stage2<L, true, 1>(b, lt, w, Y);
-      float2 *o = out + (long long)c * plane + orow;
-#pragma unroll
-      for (int k2 = 0; k2 < S::R2; ++k2)
+    if constexpr (IP)
+    {  // in place: a line's R2 stage-1 threads read all their cells, then
+       // write the twiddled values to cells k1 * R2 + lt of the same coil
+       // column; the line's threads share a warp
+      float2 a[S::R1];
+      if (lt < S::R2 && cl < CG)
       {
-        const int x = (lt + S::R1 * k2 + out_add) & (L - 1);
-        if (x < Nx)
-          o[x] = b[k2];
+#pragma unroll
+        for (int j = 0; j < S::R1; ++j)
+          a[j] = acc[acc_pos<CG, SR2>((lt + S::R2 * j + sx) & (L - 1), cl)];
+      }
+      __syncwarp();
+      if (lt < S::R2 && cl < CG)
+      {
+        fftcore::reg_fft<S::R1, fftcore::Rm<L>::V, true>(a, w);
+#pragma unroll
+        for (int k1 = 0; k1 < S::R1; ++k1)
+        {
+          float2 v = a[k1];
+          if (k1 != 0)
+          {
+            float2 r = tw[(lt * k1) & (L - 1)];
+            r.y = -r.y;
+            v = fftcore::cmul(v, r);
+          }
+          acc[acc_pos<CG, SR2>(k1 * S::R2 + lt, cl)] = v;
+        }
+      }
+      __syncwarp();
+      if (lt < S::R1 && cl < CG && c < C)
+      {
+        float2 b[S::R2];
+#pragma unroll
+        for (int t = 0; t < S::R2; ++t)
+          b[t] = acc[acc_pos<CG, SR2>(lt * S::R2 + t, cl)];
+        fftcore::reg_fft<S::R2, fftcore::Rm<L>::V, true>(b, w);
+        store(b, c);
       }
     }
-    __syncthreads();
+    else
+    {
+      float2 *Y = ex + line * S::R1 * S::YP;
+      if (lt < S::R2 && cl < CG)
+      {
+        float2 a[S::R1];
+#pragma unroll
+        for (int j = 0; j < S::R1; ++j)
+          a[j] = acc[((lt + S::R2 * j + sx) & (L - 1)) * (CG + 1) + cl];
+        fftcore::stage1<L, true, 1>(a, lt, w, tw, Y);
+      }
+      __syncthreads();
+      if (lt < S::R1 && cl < CG && c < C)
+      {
+        float2 b[S::R2];
+        fftcore::stage2<L, true, 1>(b, lt, w, Y);
+        store(b, c);
+      }
+      __syncthreads();
+    }
   }
 }
 
@@ -1305,6 +1406,236 @@ __global__ void __launch_bounds__(kThreads)
         out[(size_t)(c0 + c) * M + j] = make_float2(ax, ay);
       }
     }
+  }
+}
+
+// The same interpolation with every coil group of an item in one block (3-D,
+// used when the tiles are copied by TMA or gathered, any coil count): each
+// thread computes the footprints of its (at most two) samples once, in
+// registers, and the block walks the coil groups with two tile buffers, the
+// copy of group g + 2 issued as soon as group g's buffer is released, so
+// that the copies overlap the accumulation.  Per sample and coil the
+// arithmetic (cell order z, y, x; weight (wz * wy) * wx; one fused
+// multiply-add per cell) is that of k_forward_tma.
+constexpr int kFwdSpt = (kFwdItemSamples + kThreads - 1) / kThreads;
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
+{
+  uint32_t done = 0;
+  for (long long i = 0; i < kMbarSpin && !done; ++i)
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
+        "[%1], %2; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+  return done != 0;
+}
+
+template <int CG, int KS>
+__global__ void __launch_bounds__(kThreads, 2)
+    k_forward_tma_groups(const __grid_constant__ CUtensorMap tmap,
+                         const FwdItem *__restrict__ items,
+                         const float *__restrict__ traj,
+                         const uint32_t *__restrict__ idx,
+                         const float *__restrict__ dens,
+                         const float2 *__restrict__ grid, Geo g,
+                         const float *__restrict__ lut, uint32_t M, int C,
+                         int PX, float scale, float2 *__restrict__ out,
+                         int *__restrict__ err)
+{
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const int pad = g.pad;
+  const int cstride = pad * pad * PX;  // elements per coil
+  const int tile_elems = CG * cstride;
+  float2 *tiles = reinterpret_cast<float2 *>(smraw);
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(
+      smraw + (size_t)2 * tile_elems * sizeof(float2));
+  int &s_fail = *reinterpret_cast<int *>(mbar + 2);
+  const FwdItem it = items[blockIdx.x];
+  const int ng = (C + CG - 1) / CG;
+  int sa[3];
+  split_sector(it.sector, g, sa);
+  int base[3];
+  for (int a = 0; a < 3; ++a)
+    base[a] = sa[a] * g.sw + (g.sw >> 1) - g.offset;
+  const int x0 = base[0] & ~1;  // even start (floor, negative included)
+  const int dx = base[0] - x0;
+  bool inside = true;
+  for (int a = 0; a < 3; ++a)
+    inside = inside && base[a] >= 0 && base[a] + pad <= g.G[a];
+  const uint32_t bar0 = smem_addr(mbar), bar1 = smem_addr(mbar + 1);
+  const uint32_t tbytes = (uint32_t)(tile_elems * sizeof(float2));
+  const uint64_t tm = reinterpret_cast<uint64_t>(&tmap);
+  auto issue = [&](int gi) {  // thread 0: copy coil group gi's tile
+    const uint32_t bar = (gi & 1) ? bar1 : bar0;
+    const uint32_t dst = smem_addr(tiles + (size_t)(gi & 1) * tile_elems);
+    asm volatile(
+        "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+        "r"(tbytes)
+        : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::"
+        "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"(tm), "r"(x0), "r"(base[1]), "r"(base[2]), "r"(gi * CG), "r"(bar)
+        : "memory");
+  };
+  if (inside && threadIdx.x == 0)
+  {
+    s_fail = 0;
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0)
+                 : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1)
+                 : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    issue(0);
+    if (ng > 1)
+      issue(1);
+  }
+
+  // footprints of this thread's samples (tile frame), kept for all groups
+  int l0[kFwdSpt][3], n[kFwdSpt][3];
+  float w[kFwdSpt][3][KS];
+#pragma unroll
+  for (int s = 0; s < kFwdSpt; ++s)
+  {
+    const int t = it.begin + threadIdx.x + s * kThreads;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+    {
+      int l[KS];
+      n[s][a] = 0;
+      if (t < it.end)
+        n[s][a] = compact_axis<KS>(__ldg(traj + (size_t)a * M + t), a, sa[a],
+                                   0, g, lut, false, l, w[s][a]);
+      else
+      {
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
+          w[s][a][k] = 0.f;
+        l[0] = 0;
+      }
+      l0[s][a] = l[0];
+    }
+  }
+
+  for (int gi = 0; gi < ng; ++gi)
+  {
+    const int buf = inside ? (gi & 1) : 0;
+    const float2 *tile = tiles + (size_t)buf * tile_elems;
+    if (inside)
+    {
+      if (threadIdx.x == 0 && !mbar_wait_bounded(buf ? bar1 : bar0,
+                                                 (uint32_t)(gi >> 1) & 1u))
+        s_fail = 1;
+      __syncthreads();
+      if (s_fail)
+      {  // a copy did not complete: report, and give the copies still in
+         // flight (this group's, the next one's) a bounded wait before the
+         // block's shared memory is released
+        if (threadIdx.x == 0)
+        {
+          atomicExch(err, 1);
+          mbar_wait_bounded(buf ? bar1 : bar0, (uint32_t)(gi >> 1) & 1u);
+          if (gi + 1 < ng)
+            mbar_wait_bounded(buf ? bar0 : bar1,
+                              (uint32_t)((gi + 1) >> 1) & 1u);
+        }
+        return;
+      }
+    }
+    else
+    {  // a tile that wraps around the grid edge: plain loads
+      float2 *dst = tiles;
+      const long long G = g.grid_count;
+      for (int e = threadIdx.x; e < tile_elems; e += kThreads)
+      {
+        const int c = e / cstride;
+        int r = e - c * cstride;
+        const int z = r / (pad * PX);
+        r -= z * pad * PX;
+        const int y = r / PX, x = r - y * PX;
+        float2 v = make_float2(0.f, 0.f);
+        if (gi * CG + c < C)
+        {
+          int q[3] = {x0 + x, base[1] + y, base[2] + z};
+          for (int a = 0; a < 3; ++a)
+            q[a] = ((q[a] % g.G[a]) + g.G[a]) % g.G[a];
+          v = __ldg(grid + (long long)(gi * CG + c) * G +
+                    ((long long)q[2] * g.G[1] + q[1]) * g.G[0] + q[0]);
+        }
+        dst[e] = v;
+      }
+      __syncthreads();
+    }
+
+#pragma unroll
+    for (int s = 0; s < kFwdSpt; ++s)
+    {
+      const int t = it.begin + threadIdx.x + s * kThreads;
+      if (t >= it.end)
+        continue;
+      float2 acc[CG];
+#pragma unroll
+      for (int c = 0; c < CG; ++c)
+        acc[c] = make_float2(0.f, 0.f);
+      const int xb = l0[s][0] + dx;
+      for (int z = 0; z < n[s][2]; ++z)
+      {
+        float wzv = 0.f;
+#pragma unroll
+        for (int k = 0; k < KS; ++k)
+          if (k == z)
+            wzv = w[s][2][k];
+        for (int y = 0; y < n[s][1]; ++y)
+        {
+          float wyv = 0.f;
+#pragma unroll
+          for (int k = 0; k < KS; ++k)
+            if (k == y)
+              wyv = w[s][1][k];
+          const float wzy = __fmul_rn(wzv, wyv);
+          const int row = ((l0[s][2] + z) * pad + l0[s][1] + y) * PX + xb;
+#pragma unroll
+          for (int x = 0; x < KS; ++x)
+          {
+            if (x >= n[s][0])
+              break;
+            const float wt = __fmul_rn(wzy, w[s][0][x]);
+#pragma unroll
+            for (int c = 0; c < CG; ++c)
+            {
+              const float2 v = tile[c * cstride + row + x];
+              acc[c].x = __fmaf_rn(v.x, wt, acc[c].x);
+              acc[c].y = __fmaf_rn(v.y, wt, acc[c].y);
+            }
+          }
+        }
+      }
+      const uint32_t j = __ldg(idx + t);
+      const float sd = dens ? sqrtf(__ldg(dens + t)) : 1.0f;
+#pragma unroll
+      for (int c = 0; c < CG; ++c)
+      {
+        const int cc = gi * CG + c;
+        if (cc < C)
+        {
+          // performFFTScaling then performDensityCompensation
+          // (std_gpuNUFFT_kernels.cu:114-140, 220-242)
+          float ax = __fmul_rn(acc[c].x, scale),
+                ay = __fmul_rn(acc[c].y, scale);
+          if (dens)
+          {
+            ax = __fmul_rn(ax, sd);
+            ay = __fmul_rn(ay, sd);
+          }
+          out[(size_t)cc * M + j] = make_float2(ax, ay);
+        }
+      }
+    }
+    __syncthreads();  // this group's buffer is free
+    if (inside && threadIdx.x == 0 && gi + 2 < ng)
+      issue(gi + 2);
   }
 }
 
@@ -1872,8 +2203,27 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
           CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
-  const dim3 grd((unsigned)n_items, (unsigned)((C + cg - 1) / cg));
   const int ks = slots_for(g);
+  if (g.dim == 3 && ks == 4 && 2 * tile + 32 <= 200 * 1024)
+  {  // every coil group of an item in one block, copies double-buffered
+    const size_t smem2 = 2 * tile + 32;
+    auto launch = [&](auto kern) {
+      GN_CUDA(cudaFuncSetAttribute(
+          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+      kern<<<(unsigned)n_items, kThreads, smem2, s>>>(
+          tm, items, traj_sorted, idx, dens_sorted, grid, g, lut, M, C, PX,
+          scale, out, err);
+    };
+    switch (cg)
+    {
+    case 1: launch(k_forward_tma_groups<1, 4>); break;
+    case 2: launch(k_forward_tma_groups<2, 4>); break;
+    default: launch(k_forward_tma_groups<4, 4>); break;
+    }
+    GN_LAUNCH_CHECK("forward interpolation (tensor-copy tiles, all groups)");
+    return true;
+  }
+  const dim3 grd((unsigned)n_items, (unsigned)((C + cg - 1) / cg));
 #define GN_TMA(D, CGV, KSV)                                                    \
   {                                                                            \
     auto k = k_forward_tma<D, CGV, KSV>;                                       \
@@ -1916,11 +2266,7 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
 }
 
 
-int spmm_xfft_coils(int L)
-{
-  // accumulation rows of L x (coils + 1) complex values stay near 64 KB
-  return L <= 256 ? 32 : (L == 512 ? 16 : 8);
-}
+int spmm_xfft_coils(int L) { return xfft_max_coils(L); }
 
 bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
                               const float2 *ks, int CP, const Geo &g, int C,
@@ -1937,7 +2283,6 @@ bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
     cg = cgmax;
   if (CP % cg)
     return false;
-  const int v = cg == 32 ? 2 : 1;
   const dim3 grd((unsigned)((long long)g.G[1] * g.G[2]),
                  (unsigned)((C + cg - 1) / cg));
   bool ok = true;
@@ -1945,22 +2290,25 @@ bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
     constexpr int LL = decltype(lc)::value;
     constexpr int CGV = decltype(cgc)::value;
     constexpr int VV = decltype(vc)::value;
-    using S = fftcore::Shape<LL>;
-    constexpr int NU = kWarps * (32 / (CGV / VV));
-    const size_t head = (size_t)(LL * (CGV + 1) + LL) * sizeof(float2);
-    const size_t spread = (size_t)2 * NU * CGV * sizeof(float2) +
-                          (size_t)(LL + 1) * 4 + (size_t)2 * NU * 4;
-    const size_t exch = (size_t)S::NL * S::R1 * S::YP * sizeof(float2);
-    const size_t smem = head + (spread > exch ? spread : exch);
-    if (smem > 220 * 1024)
-    {
+    if constexpr (CGV > xfft_max_coils(LL))
+    {  // never selected (the coil group is capped above)
       ok = false;
       return;
     }
-    auto k = k_adjoint_spmm_xfft<CGV, VV, LL>;
-    GN_CUDA(cudaFuncSetAttribute(
-        k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<grd, kThreads, smem, s>>>(row_off, nz, ks, CP, g, C, roots_x, out);
+    else
+    {
+      constexpr int NU = kWarps * (32 / (CGV / VV));
+      const size_t smem = XfftLayout<CGV, LL>::smem(NU);
+      if (smem > 220 * 1024)
+      {
+        ok = false;
+        return;
+      }
+      auto k = k_adjoint_spmm_xfft<CGV, VV, LL>;
+      GN_CUDA(cudaFuncSetAttribute(
+          k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k<<<grd, kThreads, smem, s>>>(row_off, nz, ks, CP, g, C, roots_x, out);
+    }
   };
   using I = std::integral_constant<int, 1>;
   using I2 = std::integral_constant<int, 2>;

@@ -22,7 +22,9 @@ struct AdjItem
   int split;
 };
 
-// Forward work item: samples [begin, end) of one sector.
+// Forward work item: samples [begin, end) of one sector, at most
+// kFwdItemSamples of them.
+constexpr int kFwdItemSamples = 512;
 struct FwdItem
 {
   int sector;

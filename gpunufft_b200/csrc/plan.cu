@@ -42,7 +42,7 @@ thread_local std::string g_last_error;
 
 // Candidates per adjoint work item and samples per forward work item.
 constexpr int kAdjPayload = 2048;
-constexpr int kFwdPayload = 512;
+constexpr int kFwdPayload = kFwdItemSamples;
 
 // Mirrors the upstream IndPair (gpuNUFFT_types.hpp:33-49): compared by the
 // second member only, so libstdc++'s std::sort produces the upstream order.
