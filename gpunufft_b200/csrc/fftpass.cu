@@ -13,6 +13,7 @@
 
 #include "devutil.hpp"
 #include "fftcore.cuh"
+#include "tma.cuh"
 
 namespace gnufft
 {
@@ -81,6 +82,182 @@ __global__ void __launch_bounds__(Shape<L>::CT)
           dp[(long long)r * ncols] = b[k2];
       }
     }
+  }
+}
+
+// --------------------------------------------------------------------------
+// column passes with tensor-copy (TMA) tiles
+// --------------------------------------------------------------------------
+// A persistent block walks its tiles of TC adjacent columns (tile t: plane
+// t / n_ct, columns (t % n_ct) * TC ...) through two shared-memory buffers:
+// the copy of its next tile is in flight while the current one is
+// transformed.  The transform runs in place in the tile: a stage-1 thread
+// reads the rows of its residue class mod R2 and writes its twiddled
+// outputs back into rows of the same class (row k1 * R2 + residue), so no
+// thread overwrites a row another thread still has to read; after a
+// barrier, stage-2 thread k1 reads row k1 * R2 + ((u + in_add) mod R2) for
+// every stage-1 index u.  A tile row is TC * 8 = 128 bytes, so each warp
+// access covers whole rows (no bank conflicts, no padding).  The arithmetic
+// is that of k_fft_cols.
+template <int L> struct ColTma
+{
+  using S = Shape<L>;
+  static_assert(S::TC * 8 == 128, "tile rows of 128 bytes");
+  static constexpr size_t tile_bytes = (size_t)L * S::TC * sizeof(float2);
+  static size_t smem()
+  {
+    return 2 * tile_bytes + (size_t)L * sizeof(float2) + 2 * 8 + 16;
+  }
+};
+
+// One thread: expect the tile's bytes on `bar` and issue its copies (boxes
+// of box_rows rows starting at rows 0, box_rows, ...).
+__device__ __forceinline__ void col_tile_issue(const CUtensorMap *tmap,
+                                               uint32_t dst, uint32_t bar,
+                                               int col0, int plane,
+                                               int box_rows, int ncopy,
+                                               uint32_t bytes)
+{
+  tma::mbar_expect_tx(bar, bytes);
+  for (int q = 0; q < ncopy; ++q)
+    tma::copy_3d(dst + (uint32_t)(q * box_rows) * 128u, tmap, col0,
+                 q * box_rows, plane, bar);
+}
+
+// The in-place transform of column cl of tile B; returns the stage-2
+// outputs of thread lt (< R1) in b (outputs k = lt + R1 * k2).
+template <int L, bool INV>
+__device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
+                                             int in_add, int in_count,
+                                             const float2 (&w)[Rm<L>::V / 2],
+                                             const float2 *tw,
+                                             float2 (&b)[Shape<L>::R2])
+{
+  using S = Shape<L>;
+  constexpr int TC = S::TC;
+  if (lt < S::R2)
+  {
+    float2 a[S::R1];
+#pragma unroll
+    for (int j = 0; j < S::R1; ++j)
+    {
+      const int r = (lt + S::R2 * j + in_add) & (L - 1);
+      a[j] = r < in_count ? B[r * TC + cl] : make_float2(0.f, 0.f);
+    }
+    reg_fft<S::R1, Rm<L>::V, INV>(a, w);
+    const int rho = (lt + in_add) & (S::R2 - 1);
+#pragma unroll
+    for (int k1 = 0; k1 < S::R1; ++k1)
+    {
+      float2 v = a[k1];
+      if (k1 != 0)
+      {
+        float2 r = tw[(lt * k1) & (L - 1)];
+        if (INV)
+          r.y = -r.y;
+        v = cmul(v, r);
+      }
+      B[(k1 * S::R2 + rho) * TC + cl] = v;
+    }
+  }
+  __syncthreads();
+  if (lt < S::R1)
+  {
+#pragma unroll
+    for (int u = 0; u < S::R2; ++u)
+      b[u] = B[(lt * S::R2 + ((u + in_add) & (S::R2 - 1))) * TC + cl];
+    reg_fft<S::R2, Rm<L>::V, INV>(b, w);
+  }
+}
+
+template <int L, bool INV>
+__global__ void __launch_bounds__(Shape<L>::CT, 3)
+    k_fft_cols_tma(const __grid_constant__ CUtensorMap tmap,
+                   float2 *__restrict__ dst, long long ncols, long long n_ct,
+                   long long n_tiles, int box_rows, int ncopy, int dst_rows,
+                   int in_add, int in_count, int out_add, int out_count,
+                   const float2 *__restrict__ roots,
+                   const uint2 *__restrict__ colrange, int *__restrict__ err)
+{
+  using S = Shape<L>;
+  using T = ColTma<L>;
+  constexpr int TC = S::TC;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float2 *buf = reinterpret_cast<float2 *>(smraw);
+  float2 *tw = buf + 2 * L * TC;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(tw + L);
+  int &s_fail = *reinterpret_cast<int *>(mbar + 2);
+  const uint32_t bar0 = tma::smem_addr(mbar);
+  const uint32_t buf0 = tma::smem_addr(buf);
+  const uint32_t bytes = (uint32_t)(ncopy * box_rows) * 128u;
+  const long long stride = gridDim.x;
+  auto issue = [&](long long t, int b) {
+    const long long plane = t / n_ct;
+    col_tile_issue(&tmap, buf0 + (uint32_t)b * (uint32_t)T::tile_bytes,
+                   bar0 + 8u * (uint32_t)b, (int)(t - plane * n_ct) * TC,
+                   (int)plane, box_rows, ncopy, bytes);
+  };
+  if (threadIdx.x == 0)
+  {
+    s_fail = 0;
+    tma::mbar_init(bar0);
+    tma::mbar_init(bar0 + 8u);
+    tma::mbar_init_fence();
+    if (blockIdx.x < n_tiles)
+      issue(blockIdx.x, 0);
+    if (blockIdx.x + stride < n_tiles)
+      issue(blockIdx.x + stride, 1);
+  }
+  load_roots(tw, roots, L);
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  const int cl = threadIdx.x % TC, lt = threadIdx.x / TC;
+  int i = 0;
+  for (long long t = blockIdx.x; t < n_tiles; t += stride, ++i)
+  {
+    const int b = i & 1;
+    if (threadIdx.x == 0 &&
+        !tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b, (uint32_t)(i >> 1) & 1u))
+      s_fail = 1;
+    __syncthreads();
+    if (s_fail)
+    {  // a copy did not complete: report it and give the copies in flight
+       // (this tile's, the next one's) a bounded wait before returning
+      if (threadIdx.x == 0)
+      {
+        atomicExch(err, 1);
+        tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b, (uint32_t)(i >> 1) & 1u);
+        if (t + stride < n_tiles)
+          tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)(b ^ 1),
+                                 (uint32_t)((i + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    const long long plane = t / n_ct;
+    const long long col = (t - plane * n_ct) * TC + cl;
+    uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
+    if (colrange && col < ncols)
+      cr = __ldg(colrange + col);
+    const bool on = col < ncols && cr.x <= cr.y;
+    float2 bv[S::R2];
+    col_tile_fft<L, INV>(buf + (size_t)b * L * TC, cl, lt, in_add, in_count,
+                         w, tw, bv);
+    if (lt < S::R1 && on)
+    {
+      float2 *dp = dst + plane * dst_rows * ncols + col;
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int r = (lt + S::R1 * k2 + out_add) & (L - 1);
+        if (r < out_count && (unsigned)r >= cr.x && (unsigned)r <= cr.y)
+          dp[(long long)r * ncols] = bv[k2];
+      }
+    }
+    tma::fence_proxy_async();  // the in-place writes before the refill
+    __syncthreads();           // buffer b is free
+    if (threadIdx.x == 0 && t + 2 * stride < n_tiles)
+      issue(t + 2 * stride, b);
   }
 }
 
@@ -487,12 +664,73 @@ template <class K> void set_smem(K kernel, size_t bytes)
                                  (int)bytes));
 }
 
+// Tensor map of planes x rows x columns of complex values (columns
+// contiguous), box TC columns x box_rows rows x 1 plane.  False when TMA is
+// unavailable or the layout does not meet its alignment rules.
+bool col_tensor_map(CUtensorMap &tm, const float2 *base, long long ncols,
+                    int rows, long long plane_stride, long long planes, int TC,
+                    int box_rows)
+{
+  tma::EncodeTiledFn enc = tma::encode_fn();
+  if (!enc || (ncols & 1) || (plane_stride & 1) ||
+      (reinterpret_cast<uintptr_t>(base) & 15))
+    return false;
+  cuuint64_t dims[3] = {(cuuint64_t)ncols, (cuuint64_t)rows,
+                        (cuuint64_t)planes};
+  cuuint64_t strides[2] = {(cuuint64_t)ncols * sizeof(float2),
+                           (cuuint64_t)plane_stride * sizeof(float2)};
+  cuuint32_t box[3] = {(cuuint32_t)TC, (cuuint32_t)box_rows, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  return enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 3,
+             const_cast<float2 *>(base), dims, strides, box, estr,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+             CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Persistent blocks of the tensor-copy passes: three per SM.
+unsigned persistent_blocks(long long work)
+{
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess)
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const long long cap = 3LL * sms;
+  return (unsigned)(work < cap ? work : cap);
+}
+
 template <bool INV>
 void cols(int L, const float2 *src, float2 *dst, long long ncols,
           int src_rows, int dst_rows, long long planes, int in_add,
           int in_count, int out_add, int out_count, const float2 *roots,
-          cudaStream_t s, const uint2 *colrange = nullptr)
+          cudaStream_t s, const uint2 *colrange = nullptr, int *err = nullptr)
 {
+  bool done = false;
+  if (err && L <= 256)
+    with_length(L, [&](auto lc) {
+      constexpr int LL = decltype(lc)::value;
+      if constexpr (LL <= 256)
+      {
+        using S = Shape<LL>;
+        const int box_rows = src_rows < 256 ? src_rows : 256;
+        const int ncopy = (src_rows + box_rows - 1) / box_rows;
+        CUtensorMap tm;
+        if (!col_tensor_map(tm, src, ncols, src_rows,
+                            (long long)src_rows * ncols, planes, S::TC,
+                            box_rows))
+          return;
+        const long long n_ct = (ncols + S::TC - 1) / S::TC;
+        const long long n_tiles = n_ct * planes;
+        auto k = k_fft_cols_tma<LL, INV>;
+        set_smem(k, ColTma<LL>::smem());
+        k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
+            tm, dst, ncols, n_ct, n_tiles, box_rows, ncopy, dst_rows, in_add,
+            in_count, out_add, out_count, roots, colrange, err);
+        GN_LAUNCH_CHECK("pruned column transform (tensor-copy tiles)");
+        done = true;
+      }
+    });
+  if (done)
+    return;
   with_length(L, [&](auto lc) {
     constexpr int LL = decltype(lc)::value;
     using S = Shape<LL>;
@@ -547,7 +785,7 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
-                           const uint2 *zrange)
+                           const uint2 *zrange, int *err)
 {
   const long long N = g.img_count;
   const long long rows = (long long)g.N[1] * g.N[2];
@@ -583,13 +821,13 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
               (long long)C * g.N[2],
               pos_mod((long long)g.shift_inv[1] - g.crop[1], g.G[1]), g.N[1],
               pos_mod(-(long long)g.shift_fwd[1], g.G[1]), g.G[1], roots[1],
-              s);
+              s, nullptr, err);
   if (g.dim == 3)  // z: B -> grid
     cols<false>(g.G[2], tmp_b, grid, (long long)g.G[1] * g.G[0], g.N[2],
                 g.G[2], C,
                 pos_mod((long long)g.shift_inv[2] - g.crop[2], g.G[2]),
                 g.N[2], pos_mod(-(long long)g.shift_fwd[2], g.G[2]), g.G[2],
-                roots[2], s, zrange);
+                roots[2], s, zrange, err);
 }
 
 void launch_pruned_adjoint(const float2 *grid, const float *deapo,
@@ -652,7 +890,7 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
                                   int stage, int accumulate,
                                   const float2 *const roots[3],
                                   float2 *tmp_b, float2 *part, float2 *out,
-                                  cudaStream_t s)
+                                  cudaStream_t s, int *err)
 {
   const long long N = g.img_count;
   const float2 *src = xrows;
@@ -663,7 +901,7 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
     cols<true>(g.G[1], xrows, tmp_b, g.N[0], g.G[1], g.N[1],
                (long long)C * g.G[2], 0, g.G[1],
                pos_mod(-(long long)g.crop[1] - g.shift_inv[1], g.G[1]),
-               g.N[1], roots[1], s);
+               g.N[1], roots[1], s, nullptr, err);
     src = tmp_b;
     ncols = (long long)g.N[1] * g.N[0];
     ax = 2;

@@ -45,11 +45,14 @@ size_t pruned_scratch_b(const Geo &g, int C);
 // roots[a]: the root table of axis a (length G[a]).
 // zrange (3-D, optional): per (y, x) column the z rows to write; the
 // others are left as they are (the interpolation never reads them).
+// err (optional): the mapped error flag of the tensor-copy passes (set when
+// a tile copy does not complete within its bounded wait); without it the
+// passes load their tiles with plain loads.
 void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
-                           const uint2 *zrange = nullptr);
+                           const uint2 *zrange = nullptr, int *err = nullptr);
 
 // Adjoint: grid [C][G] (INVERSE fftshift folded in by the adjoint spread)
 // -> unnormalised inverse DFT -> crop of the second INVERSE fftshift ->
@@ -72,7 +75,7 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
                                   int stage, int accumulate,
                                   const float2 *const roots[3],
                                   float2 *tmp_b, float2 *part, float2 *out,
-                                  cudaStream_t s);
+                                  cudaStream_t s, int *err = nullptr);
 size_t pruned_scratch_xfirst(const Geo &g, int C);
 
 }  // namespace gnufft

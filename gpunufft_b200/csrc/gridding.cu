@@ -27,6 +27,7 @@
 #include "devutil.hpp"
 #include "fftcore.cuh"
 #include "footprint.cuh"
+#include "tma.cuh"
 
 namespace gnufft
 {
@@ -938,8 +939,9 @@ __global__ void __launch_bounds__(kThreads, L <= 256 ? 3 : 1)
   float2 w[fftcore::Rm<L>::V / 2];
   fftcore::load_reg_roots<L>(w, tw);
   const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
-  // FFT input n holds the cell stored at n: logical x = (n + floor(G/2))
-  const int sx = g.shift_inv[0];
+  // FFT input n holds the cell stored at n: logical x = (n + floor(G/2)),
+  // G = L a power of two (the launcher checks shift_inv[0] == L / 2)
+  constexpr int sx = L / 2;
   // FFT output k holds image x = (k - crop - floor(G/2)) mod G when < N
   int out_add = (-(g.crop[0] + g.shift_inv[0])) % L;
   if (out_add < 0)
@@ -1223,12 +1225,9 @@ __global__ void __launch_bounds__(kThreads)
 // gathered with plain loads instead.  Then every thread takes one sample:
 // its per-axis footprint (tile frame, upstream arithmetic) in registers,
 // and for each footprint cell the CG coil values of the tile.
-constexpr long long kMbarSpin = 1LL << 22;  // bounded wait for the copy
-
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
+using tma::kMbarSpin;
+using tma::mbar_wait_bounded;
+using tma::smem_addr;
 
 template <int DIM, int CG, int KS>
 __global__ void __launch_bounds__(kThreads)
@@ -1410,30 +1409,19 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // The same interpolation with every coil group of an item in one block (3-D,
-// used when the tiles are copied by TMA or gathered, any coil count): each
-// thread computes the footprints of its (at most two) samples once, in
-// registers, and the block walks the coil groups with two tile buffers, the
-// copy of group g + 2 issued as soon as group g's buffer is released, so
-// that the copies overlap the accumulation.  Per sample and coil the
-// arithmetic (cell order z, y, x; weight (wz * wy) * wx; one fused
+// tiles copied by TMA or, where they wrap, gathered): each thread computes
+// the footprints of its (at most two) samples once, in registers, and the
+// block walks the coil groups through a ring of `nbuf` tile buffers; the
+// copy of group g + nbuf is issued as soon as group g's buffer is released,
+// so nbuf - 1 copies overlap each group's accumulation.  Per sample and coil
+// the arithmetic (cell order z, y, x; weight (wz * wy) * wx; one fused
 // multiply-add per cell) is that of k_forward_tma.
+// Shared memory: nbuf tiles [CG][pad][pad][PX] | nbuf mbarriers | flag.
 constexpr int kFwdSpt = (kFwdItemSamples + kThreads - 1) / kThreads;
+constexpr int kFwdMaxBufs = 8;
 
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity)
-{
-  uint32_t done = 0;
-  for (long long i = 0; i < kMbarSpin && !done; ++i)
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
-        "[%1], %2; selp.u32 %0, 1, 0, p; }"
-        : "=r"(done)
-        : "r"(bar), "r"(parity)
-        : "memory");
-  return done != 0;
-}
-
-template <int CG, int KS>
-__global__ void __launch_bounds__(kThreads, 2)
+template <int CG, int KS, int MINB>
+__global__ void __launch_bounds__(kThreads, MINB)
     k_forward_tma_groups(const __grid_constant__ CUtensorMap tmap,
                          const FwdItem *__restrict__ items,
                          const float *__restrict__ traj,
@@ -1441,8 +1429,8 @@ __global__ void __launch_bounds__(kThreads, 2)
                          const float *__restrict__ dens,
                          const float2 *__restrict__ grid, Geo g,
                          const float *__restrict__ lut, uint32_t M, int C,
-                         int PX, float scale, float2 *__restrict__ out,
-                         int *__restrict__ err)
+                         int PX, int nbuf, float scale,
+                         float2 *__restrict__ out, int *__restrict__ err)
 {
   extern __shared__ __align__(128) unsigned char smraw[];
   const int pad = g.pad;
@@ -1450,8 +1438,8 @@ __global__ void __launch_bounds__(kThreads, 2)
   const int tile_elems = CG * cstride;
   float2 *tiles = reinterpret_cast<float2 *>(smraw);
   uint64_t *mbar = reinterpret_cast<uint64_t *>(
-      smraw + (size_t)2 * tile_elems * sizeof(float2));
-  int &s_fail = *reinterpret_cast<int *>(mbar + 2);
+      smraw + (size_t)nbuf * tile_elems * sizeof(float2));
+  int &s_fail = *reinterpret_cast<int *>(mbar + nbuf);
   const FwdItem it = items[blockIdx.x];
   const int ng = (C + CG - 1) / CG;
   int sa[3];
@@ -1464,12 +1452,13 @@ __global__ void __launch_bounds__(kThreads, 2)
   bool inside = true;
   for (int a = 0; a < 3; ++a)
     inside = inside && base[a] >= 0 && base[a] + pad <= g.G[a];
-  const uint32_t bar0 = smem_addr(mbar), bar1 = smem_addr(mbar + 1);
+  const uint32_t bar_base = smem_addr(mbar);
   const uint32_t tbytes = (uint32_t)(tile_elems * sizeof(float2));
   const uint64_t tm = reinterpret_cast<uint64_t>(&tmap);
   auto issue = [&](int gi) {  // thread 0: copy coil group gi's tile
-    const uint32_t bar = (gi & 1) ? bar1 : bar0;
-    const uint32_t dst = smem_addr(tiles + (size_t)(gi & 1) * tile_elems);
+    const int b = gi % nbuf;
+    const uint32_t bar = bar_base + 8u * (uint32_t)b;
+    const uint32_t dst = smem_addr(tiles + (size_t)b * tile_elems);
     asm volatile(
         "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
         "r"(tbytes)
@@ -1483,14 +1472,13 @@ __global__ void __launch_bounds__(kThreads, 2)
   if (inside && threadIdx.x == 0)
   {
     s_fail = 0;
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar0)
-                 : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar1)
-                 : "memory");
+    for (int b = 0; b < nbuf; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(
+                       bar_base + 8u * (uint32_t)b)
+                   : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    issue(0);
-    if (ng > 1)
-      issue(1);
+    for (int gi = 0; gi < nbuf && gi < ng; ++gi)
+      issue(gi);
   }
 
   // footprints of this thread's samples (tile frame), kept for all groups
@@ -1521,25 +1509,26 @@ __global__ void __launch_bounds__(kThreads, 2)
 
   for (int gi = 0; gi < ng; ++gi)
   {
-    const int buf = inside ? (gi & 1) : 0;
+    const int buf = inside ? gi % nbuf : 0;
     const float2 *tile = tiles + (size_t)buf * tile_elems;
     if (inside)
     {
-      if (threadIdx.x == 0 && !mbar_wait_bounded(buf ? bar1 : bar0,
-                                                 (uint32_t)(gi >> 1) & 1u))
+      // the k-th use of a buffer completes phase k of its barrier
+      if (threadIdx.x == 0 &&
+          !mbar_wait_bounded(bar_base + 8u * (uint32_t)buf,
+                             (uint32_t)(gi / nbuf) & 1u))
         s_fail = 1;
       __syncthreads();
       if (s_fail)
       {  // a copy did not complete: report, and give the copies still in
-         // flight (this group's, the next one's) a bounded wait before the
+         // flight (groups gi .. gi + nbuf - 1) a bounded wait before the
          // block's shared memory is released
         if (threadIdx.x == 0)
         {
           atomicExch(err, 1);
-          mbar_wait_bounded(buf ? bar1 : bar0, (uint32_t)(gi >> 1) & 1u);
-          if (gi + 1 < ng)
-            mbar_wait_bounded(buf ? bar0 : bar1,
-                              (uint32_t)((gi + 1) >> 1) & 1u);
+          for (int q = gi; q < ng && q < gi + nbuf; ++q)
+            mbar_wait_bounded(bar_base + 8u * (uint32_t)(q % nbuf),
+                              (uint32_t)(q / nbuf) & 1u);
         }
         return;
       }
@@ -1634,8 +1623,8 @@ __global__ void __launch_bounds__(kThreads, 2)
       }
     }
     __syncthreads();  // this group's buffer is free
-    if (inside && threadIdx.x == 0 && gi + 2 < ng)
-      issue(gi + 2);
+    if (inside && threadIdx.x == 0 && gi + nbuf < ng)
+      issue(gi + nbuf);
   }
 }
 
@@ -2119,32 +2108,8 @@ void launch_forward_interp(const FwdItem *items, int n_items,
 }
 
 
-// Tensor-map encoding through the driver entry point (no link-time
-// dependency on the driver library).
-namespace
-{
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType,
-                                  cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *,
-                                  const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion,
-                                  CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn()
-{
-  static EncodeTiledFn fn = [] {
-    void *f = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f,
-                                cudaEnableDefault, &q) != cudaSuccess ||
-        q != cudaDriverEntryPointSuccess)
-      return (EncodeTiledFn) nullptr;
-    return reinterpret_cast<EncodeTiledFn>(f);
-  }();
-  return fn;
-}
-}  // namespace
+using tma::EncodeTiledFn;
+using tma::encode_fn;
 
 bool launch_forward_interp_tma(const FwdItem *items, int n_items,
                                const float *traj_sorted, const uint32_t *idx,
@@ -2204,21 +2169,36 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
   const int ks = slots_for(g);
-  if (g.dim == 3 && ks == 4 && 2 * tile + 32 <= 200 * 1024)
-  {  // every coil group of an item in one block, copies double-buffered
-    const size_t smem2 = 2 * tile + 32;
+  if (g.dim == 3 && ks == 4 && 2 * tile + 128 <= 200 * 1024)
+  {  // every coil group of an item in one block: a ring of tile buffers,
+     // as many as fit three blocks per SM (74 KB), at least two
+    int nbuf = (int)((74 * 1024 - 128) / tile);
+    nbuf = std::max(2, std::min(nbuf, kFwdMaxBufs));
+    const int ng = (C + cg - 1) / cg;
+    nbuf = std::min(nbuf, std::max(2, ng));
+    const size_t smem2 = (size_t)nbuf * tile + 8 * nbuf + 16;
+    const bool three = smem2 <= 74 * 1024;
     auto launch = [&](auto kern) {
       GN_CUDA(cudaFuncSetAttribute(
           kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
       kern<<<(unsigned)n_items, kThreads, smem2, s>>>(
           tm, items, traj_sorted, idx, dens_sorted, grid, g, lut, M, C, PX,
-          scale, out, err);
+          nbuf, scale, out, err);
     };
     switch (cg)
     {
-    case 1: launch(k_forward_tma_groups<1, 4>); break;
-    case 2: launch(k_forward_tma_groups<2, 4>); break;
-    default: launch(k_forward_tma_groups<4, 4>); break;
+    case 1:
+      if (three) launch(k_forward_tma_groups<1, 4, 3>);
+      else launch(k_forward_tma_groups<1, 4, 2>);
+      break;
+    case 2:
+      if (three) launch(k_forward_tma_groups<2, 4, 3>);
+      else launch(k_forward_tma_groups<2, 4, 2>);
+      break;
+    default:
+      if (three) launch(k_forward_tma_groups<4, 4, 3>);
+      else launch(k_forward_tma_groups<4, 4, 2>);
+      break;
     }
     GN_LAUNCH_CHECK("forward interpolation (tensor-copy tiles, all groups)");
     return true;
@@ -2274,7 +2254,7 @@ bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
                               cudaStream_t s)
 {
   const int L = g.G[0];
-  if (L < 16 || L > 1024 || (L & (L - 1)))
+  if (L < 16 || L > 1024 || (L & (L - 1)) || g.shift_inv[0] != L / 2)
     return false;
   const int cgmax = spmm_xfft_coils(L);
   // the spread's coil group must divide the k-space lane count CP

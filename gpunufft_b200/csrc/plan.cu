@@ -544,6 +544,17 @@ void check_coils(const gnufft_plan &p, uint32_t C)
 }
 
 // Root tables (once) and grow-only scratch of the pruned transforms.
+// A tile copy of an earlier call that did not complete within its bounded
+// wait set the mapped flag: report it (once) instead of computing on.
+void check_copy_err(gnufft_plan &p)
+{
+  if (p.copy_err_h && *(volatile int *)p.copy_err_h)
+  {
+    *p.copy_err_h = 0;
+    throw Error(kCudaError, "a tile copy did not complete within its wait");
+  }
+}
+
 void ensure_pruned(gnufft_plan &p, uint32_t C, cudaStream_t s)
 {
   for (int a = 0; a < p.g.dim; ++a)
@@ -598,6 +609,7 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
   if (p.pruned && !conv)
   {  // spread whole grid rows with the inverse x transform fused (the grid
      // buffer receives only the cropped x outputs), then y and z
+    check_copy_err(p);
     ensure_pruned(p, C, s);
     if (launch_adjoint_spmm_xfft(p.w_rows.as<uint32_t>(), p.w_nz.as<uint2>(),
                                  p.ks.as<float2>(), CP, g, (int)C,
@@ -610,7 +622,7 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
           grid, p.deapo.as<float>(),
           stage == GNUFFT_DEAPODIZATION ? sens : nullptr, g, (int)C,
           stage == GNUFFT_FFT ? 1 : 2, accumulate, root_ptrs(p).data(),
-          p.fft_b.as<float2>(), p.fft_a.as<float2>(), img, s);
+          p.fft_b.as<float2>(), p.fft_a.as<float2>(), img, s, p.copy_err_d);
       p.launches += g.dim - 1;
       p.mark(5, s);
       p.mark(6, s);
@@ -675,12 +687,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
   const bool dens_est = stage == GNUFFT_DENSITY_ESTIMATION;
   if (p.pruned && !dens_est)
   {  // sens, deapodization, pad, shift and the transform in g.dim passes
-    if (*(volatile int *)p.copy_err_h)
-    {
-      *p.copy_err_h = 0;
-      throw Error(kCudaError,
-                  "a forward tile copy did not complete within its wait");
-    }
+    check_copy_err(p);
     ensure_pruned(p, C, s);
     p.mark(0, s);
     p.mark(1, s);
@@ -688,7 +695,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
     launch_pruned_forward(img, sens, p.deapo.as<float>(), g, (int)C,
                           root_ptrs(p).data(), p.fft_a.as<float2>(),
                           p.fft_b.as<float2>(), grid, s,
-                          p.zrange.as<uint2>());
+                          p.zrange.as<uint2>(), p.copy_err_d);
     p.launches += g.dim;
     p.mark(5, s);
     p.mark(2, s);
