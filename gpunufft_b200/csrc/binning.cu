@@ -192,27 +192,6 @@ __global__ void k_gather(const float *__restrict__ traj,
   }
 }
 
-// Distinct owner sectors (cell / sw) of the footprint cells along one axis.
-__device__ __forceinline__ int axis_owners(float c, int ax, int sec_ax,
-                                           const Geo &g, const float *lut,
-                                           int *owners)
-{
-  int cells[kSlots];
-  float w[kSlots];
-  const int n = axis_footprint(c, ax, sec_ax, g, lut, cells, w);
-  int k = 0;
-  for (int i = 0; i < n; ++i)
-  {
-    const int o = cells[i] / g.sw;
-    bool seen = false;
-    for (int j = 0; j < k; ++j)
-      seen |= owners[j] == o;
-    if (!seen)
-      owners[k++] = o;
-  }
-  return k;
-}
-
 __device__ __forceinline__ void split_sector(uint32_t s, const Geo &g,
                                              int *sa)
 {
@@ -220,45 +199,6 @@ __device__ __forceinline__ void split_sector(uint32_t s, const Geo &g,
   uint32_t r = s / (uint32_t)g.S[0];
   sa[1] = (int)(r % (uint32_t)g.S[1]);
   sa[2] = (int)(r / (uint32_t)g.S[1]);
-}
-
-template <bool FILL>
-__global__ void k_owner_pairs(const float *__restrict__ traj_sorted,
-                              const uint32_t *__restrict__ sector_sorted,
-                              uint32_t M, Geo g, const float *__restrict__ lut,
-                              uint32_t *__restrict__ count,
-                              const uint32_t *__restrict__ pos,
-                              uint32_t *__restrict__ keys,
-                              uint32_t *__restrict__ vals)
-{
-  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < M;
-       t += (size_t)gridDim.x * blockDim.x)
-  {
-    int sa[3];
-    split_sector(sector_sorted[t], g, sa);
-    int own[3][kSlots];
-    int no[3] = {1, 1, 1};
-    own[2][0] = 0;
-    for (int a = 0; a < g.dim; ++a)
-      no[a] = axis_owners(traj_sorted[(size_t)a * M + t], a, sa[a], g, lut,
-                          own[a]);
-    if (!FILL)
-    {
-      count[t] = (uint32_t)(no[0] * no[1] * no[2]);
-      continue;
-    }
-    uint32_t p = pos[t];
-    for (int z = 0; z < no[2]; ++z)
-      for (int y = 0; y < no[1]; ++y)
-        for (int x = 0; x < no[0]; ++x)
-        {
-          keys[p] = (uint32_t)own[0][x] +
-                    (uint32_t)g.S[0] *
-                        ((uint32_t)own[1][y] + (uint32_t)g.S[1] * own[2][z]);
-          vals[p] = (uint32_t)t;
-          ++p;
-        }
-  }
 }
 
 // Every (cell, weight) of the footprint of sorted sample t.
@@ -416,51 +356,6 @@ void gather_sorted(const float *traj, const float *dens, const uint32_t *idx,
   k_gather<<<grid_for(M, 256, 8192), 256, 0, s>>>(traj, dens, idx, M, dim,
                                                   traj_sorted, dens_sorted);
   GN_LAUNCH_CHECK("gather sorted");
-}
-
-size_t build_owner_candidates(const float *traj_sorted,
-                              const uint32_t *sector_sorted, uint32_t M,
-                              const Geo &g, const float *lut,
-                              DeviceBuffer &cand, DeviceBuffer &cand_offsets,
-                              cudaStream_t s)
-{
-  const uint32_t S = (uint32_t)g.n_sectors;
-  cand_offsets.reset((size_t)(S + 1) * sizeof(uint32_t));
-  if (M == 0)
-  {
-    GN_CUDA(cudaMemsetAsync(cand_offsets.get(), 0,
-                            (size_t)(S + 1) * sizeof(uint32_t), s));
-    cand.reset(sizeof(uint32_t));
-    return 0;
-  }
-  DeviceBuffer count((size_t)(M + 1) * sizeof(uint32_t));
-  GN_CUDA(cudaMemsetAsync(count.get(), 0, (size_t)(M + 1) * sizeof(uint32_t),
-                          s));
-  const unsigned nb = grid_for(M, 256, 8192);
-  k_owner_pairs<false><<<nb, 256, 0, s>>>(traj_sorted, sector_sorted, M, g,
-                                          lut, count.as<uint32_t>(), nullptr,
-                                          nullptr, nullptr);
-  GN_LAUNCH_CHECK("owner count");
-  scan_exclusive(count.as<uint32_t>(), count.as<uint32_t>(), (size_t)M + 1,
-                 s);
-  uint32_t total = 0;
-  GN_CUDA(cudaMemcpyAsync(&total, count.as<uint32_t>() + M, sizeof(uint32_t),
-                          cudaMemcpyDeviceToHost, s));
-  GN_CUDA(cudaStreamSynchronize(s));
-  DeviceBuffer keys((size_t)total * sizeof(uint32_t) + 4);
-  DeviceBuffer vals((size_t)total * sizeof(uint32_t) + 4);
-  k_owner_pairs<true><<<nb, 256, 0, s>>>(
-      traj_sorted, sector_sorted, M, g, lut, nullptr, count.as<uint32_t>(),
-      keys.as<uint32_t>(), vals.as<uint32_t>());
-  GN_LAUNCH_CHECK("owner fill");
-  DeviceBuffer skeys((size_t)total * sizeof(uint32_t) + 4);
-  cand.reset((size_t)total * sizeof(uint32_t) + 4);
-  sort_pairs(keys.as<uint32_t>(), vals.as<uint32_t>(), skeys.as<uint32_t>(),
-             cand.as<uint32_t>(), total, bits_for(S ? S - 1 : 0), s);
-  histogram_offsets(skeys.as<uint32_t>(), total, S,
-                    cand_offsets.as<uint32_t>(), s);
-  GN_CUDA(cudaStreamSynchronize(s));
-  return total;
 }
 
 size_t build_interp_matrix(const float *traj_sorted,

@@ -1,5 +1,5 @@
 // Plan-time integer work on the device: sector assignment, stable sort,
-// scans and the per-sector owner candidate lists.
+// scans, the interpolation matrix and the forward column ranges.
 #pragma once
 
 #include <cstdint>
@@ -36,17 +36,6 @@ void assign_sectors(const float *traj, uint32_t M, const Geo &g,
 void gather_sorted(const float *traj, const float *dens, const uint32_t *idx,
                    uint32_t M, int dim, float *traj_sorted, float *dens_sorted,
                    cudaStream_t s);
-
-// Owner candidate lists for the adjoint: for every sector T, the sorted
-// samples whose kernel footprint touches a grid cell owned by T (the cells
-// T*sw .. T*sw+sw-1 per axis, after wrap-around).  Output: cand (values =
-// sorted sample index, grouped by T, ascending within T) and
-// cand_offsets[S + 1].  Returns the number of (sample, owner) pairs.
-size_t build_owner_candidates(const float *traj_sorted,
-                              const uint32_t *sector_sorted, uint32_t M,
-                              const Geo &g, const float *lut,
-                              DeviceBuffer &cand, DeviceBuffer &cand_offsets,
-                              cudaStream_t s);
 
 // Interpolation matrix of the trajectory in CSR form keyed by grid cell:
 // for every (unshifted, x-fastest) grid cell the list of (sorted sample t,

@@ -58,13 +58,6 @@ __device__ __forceinline__ void cp_async8(void *smem_dst, const void *gsrc)
                "l"(gsrc)
                : "memory");
 }
-__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gsrc)
-{
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s),
-               "l"(gsrc)
-               : "memory");
-}
 __device__ __forceinline__ void cp_async_wait_all()
 {
   asm volatile("cp.async.wait_all;\n" ::: "memory");
@@ -124,15 +117,11 @@ __global__ void __launch_bounds__(kThreads)
 // compact per-axis footprints (phase A: one sample per thread)
 // --------------------------------------------------------------------------
 // An axis is described by up to KS (index, weight) entries with static
-// register indices.  Tile frame (forward): the entries are the consecutive
-// cells imin.. of the sample's own tile.  Owner frame (adjoint): the cells,
-// after wrap-around, that lie in the target's sw owned cells, as indices
-// relative to the target's first cell (on grids smaller than a tile plus a
-// footprint these need not be consecutive).
+// register indices: the consecutive cells imin.. of the footprint in the
+// frame of the sample's own sector tile.
 template <int KS>
 __device__ __forceinline__ int compact_axis(float c, int ax, int sec_ax,
-                                            int tgt_ax, const Geo &g,
-                                            const float *lut, bool owner,
+                                            const Geo &g, const float *lut,
                                             int *li, float *w)
 {
   const int center = sec_ax * g.sw + (g.sw >> 1);
@@ -149,8 +138,6 @@ __device__ __forceinline__ int compact_axis(float c, int ax, int sec_ax,
     imax = pmax;
   if (imin >= pmax)
     imin = (int)(pmax - 2 * g.kernel_radius);
-  const int G = g.G[ax];
-  const int o = tgt_ax * g.sw;
   int n = 0;
 #pragma unroll
   for (int k = 0; k < KS; ++k)
@@ -177,21 +164,12 @@ __device__ __forceinline__ int compact_axis(float c, int ax, int sec_ax,
       lx = lx < 0 ? 0 : (lx > g.lut_len - 1 ? g.lut_len - 1 : lx);
       wt = valid ? __ldg(lut + lx) : 0.0f;
     }
-    int cell = i;  // tile frame
-    if (owner)
-    {
-      int gw = wrap_mod(gc, G);
-      if (gw < 0 || gw >= G)
-        gw = ((gc % G) + G) % G;
-      cell = gw - o;
-      valid = valid && cell >= 0 && cell < g.sw;
-    }
     // append (static indices only: entry j receives candidate k if j == n)
 #pragma unroll
     for (int j = 0; j < KS; ++j)
       if (valid && j == n)
       {
-        li[j] = cell;
+        li[j] = i;
         w[j] = wt;
       }
     n += valid ? 1 : 0;
@@ -199,359 +177,9 @@ __device__ __forceinline__ int compact_axis(float c, int ax, int sec_ax,
   return n;
 }
 
-// --------------------------------------------------------------------------
-// adjoint owner spread
-// --------------------------------------------------------------------------
-// Planes of the owned cells (z in 3-D, y rows in 2-D) are grouped in
-// buckets p % 32; unit u (a warp slot of CG coil lanes) owns the buckets
-// b % NU == u, so no two units ever touch the same cell and the shared
-// tile is updated with plain loads and stores.  Phase A lists, per bucket,
-// the (candidate, plane entry) pairs of the chunk in candidate order (warp
-// ballots, deterministic), so phase B visits only its own work.
-//
-// Shared memory: [tile: sw^DIM cells x (CG+1) float2]
-//   [t: CH ints][counts: DIM x CH][indices: DIM x KS x CH]
-//   [weights: DIM x KS x CH floats][lists: NB x CH u16][list counts: NB]
-//   [per-warp bucket counts: NB x 16][k-space rows of the chunk: CH x CG]
-constexpr int kMaxBuckets = 32;
-
-template <int DIM, int CG, int KS>
-__global__ void __launch_bounds__(512)
-    k_adjoint_spread(const AdjItem *__restrict__ items,
-                     const uint32_t *__restrict__ cand,
-                     const uint32_t *__restrict__ sector_sorted,
-                     const float *__restrict__ traj,
-                     const float2 *__restrict__ ks, int CP, Geo g,
-                     const float *__restrict__ lut, uint32_t M, int C,
-                     int shift, int CH, float2 *__restrict__ grid)
-{
-  extern __shared__ float2 smem[];
-  constexpr int SLOTS = 32 / CG;
-  constexpr int PITCH = CG + 1;
-  constexpr int PA = DIM - 1;  // plane axis: z in 3-D, y in 2-D
-  const AdjItem it = items[blockIdx.x];
-  const int group = blockIdx.y;
-  const int sw = g.sw;
-  const int cells = DIM == 3 ? sw * sw * sw : sw * sw;
-  const int nthreads = blockDim.x;  // CH <= nthreads candidates per chunk
-  const int nwarps = nthreads >> 5;
-  const int NB = sw < kMaxBuckets ? sw : kMaxBuckets;
-  float2 *tile = smem;
-  int *s_t = reinterpret_cast<int *>(smem + (size_t)cells * PITCH);
-  int *s_n = s_t + CH;             // [DIM][CH]
-  int *s_l = s_n + DIM * CH;       // [DIM][KS][CH]
-  float *s_w = reinterpret_cast<float *>(s_l + DIM * KS * CH);
-  unsigned short *s_list =
-      reinterpret_cast<unsigned short *>(s_w + DIM * KS * CH);  // [NB][CH]
-  int *s_cnt = reinterpret_cast<int *>(s_list + NB * CH + (NB * CH & 1));
-  int *s_wc = s_cnt + NB;          // [NB][16]
-  float2 *s_v = reinterpret_cast<float2 *>(
-      reinterpret_cast<uintptr_t>(s_wc + NB * 16 + 3) & ~uintptr_t(15));
-  {
-    float4 *t4 = reinterpret_cast<float4 *>(tile);
-    const int n4 = (cells * PITCH) / 2;
-    for (int i = threadIdx.x; i < n4; i += nthreads)
-      t4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if ((cells * PITCH) & 1)
-      tile[cells * PITCH - 1] = make_float2(0.f, 0.f);
-  }
-  int ta[3];
-  split_sector(it.target, g, ta);
-
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int slot = lane / CG, coil = lane % CG;
-  const int unit = warp * SLOTS + slot;
-  const int NU = nwarps * SLOTS;
-  const unsigned lt = (1u << lane) - 1u;
-
-  for (int base = it.begin; base < it.end; base += CH)
-  {
-    __syncthreads();  // previous chunk consumed, tile zeroed
-    // ---- phase A: footprints of the chunk's candidates, one per thread
-    unsigned bucket_mask = 0;
-    int bucket_entry[KS];
-    {
-      const int j = base + threadIdx.x;
-      const bool holder = threadIdx.x < CH;
-      int t = 0;
-      int nn[3] = {0, 0, 0};
-      int l[3][KS];
-      float w[3][KS];
-#pragma unroll
-      for (int a = 0; a < 3; ++a)
-#pragma unroll
-        for (int k = 0; k < KS; ++k)
-        {
-          l[a][k] = 0;
-          w[a][k] = 0.f;
-        }
-      if (holder && j < it.end)
-      {
-        t = (int)cand[j];
-        int sa[3];
-        split_sector((int)sector_sorted[t], g, sa);
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-          nn[a] = compact_axis<KS>(traj[(size_t)a * M + t], a, sa[a], ta[a],
-                                   g, lut, true, l[a], w[a]);
-      }
-      if (holder)
-      {
-        s_t[threadIdx.x] = t;
-#pragma unroll
-        for (int a = 0; a < DIM; ++a)
-        {
-          s_n[a * CH + threadIdx.x] = nn[a];
-#pragma unroll
-          for (int k = 0; k < KS; ++k)
-          {
-            s_l[(a * KS + k) * CH + threadIdx.x] = l[a][k];
-            s_w[(a * KS + k) * CH + threadIdx.x] = w[a][k];
-          }
-        }
-      }
-      // an owned footprint spans < sw consecutive planes, so each bucket
-      // holds at most one of this candidate's planes
-#pragma unroll
-      for (int k = 0; k < KS; ++k)
-        if (k < nn[PA])
-        {
-          const int b = l[PA][k] % kMaxBuckets;
-          bucket_mask |= 1u << b;
-        }
-#pragma unroll
-      for (int k = 0; k < KS; ++k)
-        bucket_entry[k] = l[PA][k] % kMaxBuckets;
-      for (int b = 0; b < NB; ++b)
-      {
-        const unsigned ball = __ballot_sync(0xffffffffu, (bucket_mask >> b) & 1u);
-        if (lane == 0)
-          s_wc[b * 16 + warp] = __popc(ball);
-      }
-      __syncthreads();
-      // stage the chunk's k-space rows (this coil group) in shared memory
-      {
-        const int nck = min(CH, it.end - base);
-        constexpr int V4 = CG >= 2 ? CG / 2 : 1;  // 16-byte pieces per row
-        for (int q = threadIdx.x; q < nck * V4; q += nthreads)
-        {
-          const int r = q / V4, k = q - r * V4;
-          const float2 *src = ks + (size_t)s_t[r] * CP + group * CG;
-          if (CG >= 2)
-            cp_async16(s_v + r * CG + 2 * k, src + 2 * k);
-          else
-            cp_async8(s_v + r * CG, src);
-        }
-      }
-      if (threadIdx.x < NB)
-      {
-        const int b = threadIdx.x;
-        int acc = 0;
-        for (int w2 = 0; w2 < nwarps; ++w2)
-        {
-          const int c2 = s_wc[b * 16 + w2];
-          s_wc[b * 16 + w2] = acc;
-          acc += c2;
-        }
-        s_cnt[b] = acc;
-      }
-      __syncthreads();
-      for (int b = 0; b < NB; ++b)
-      {
-        const unsigned ball = __ballot_sync(0xffffffffu, (bucket_mask >> b) & 1u);
-        if ((bucket_mask >> b) & 1u)
-        {
-          int e = 0;
-#pragma unroll
-          for (int k = 0; k < KS; ++k)
-            if (k < nn[PA] && bucket_entry[k] == b)
-              e = k;
-          const int pos = s_wc[b * 16 + warp] + __popc(ball & lt);
-          s_list[b * CH + pos] = (unsigned short)((threadIdx.x << 3) | e);
-        }
-      }
-      cp_async_wait_all();
-    }
-    __syncthreads();
-    // ---- phase B: unit u works through the lists of its buckets
-    for (int b = unit; b < NB; b += NU)
-    {
-      const int cnt = s_cnt[b];
-      for (int q = 0; q < cnt; ++q)
-      {
-        const int entry = s_list[b * CH + q];
-        const int i = entry >> 3, e = entry & 7;
-        const int p = s_l[(PA * KS + e) * CH + i];
-        const float wp = s_w[(PA * KS + e) * CH + i];
-        const float2 v = s_v[i * CG + coil];
-        const int nx = s_n[i];
-        int lx[KS];
-        float wx[KS];
-#pragma unroll
-        for (int k = 0; k < KS; ++k)
-        {
-          lx[k] = s_l[k * CH + i];
-          wx[k] = s_w[k * CH + i];
-        }
-        const int ny = DIM == 3 ? s_n[CH + i] : 1;
-        for (int yy = 0; yy < ny; ++yy)
-        {
-          // upstream weight order: (K[z] * K[y]) * K[x]
-          const float wzy =
-              DIM == 3 ? __fmul_rn(wp, s_w[(KS + yy) * CH + i]) : wp;
-          const int row = DIM == 3 ? p * sw + s_l[(KS + yy) * CH + i] : p;
-          float2 *trow = tile + (size_t)row * sw * PITCH + coil;
-          float2 acc[KS];
-#pragma unroll
-          for (int xx = 0; xx < KS; ++xx)
-            if (xx < nx)
-              acc[xx] = trow[(size_t)lx[xx] * PITCH];
-#pragma unroll
-          for (int xx = 0; xx < KS; ++xx)
-            if (xx < nx)
-            {
-              const float wt = __fmul_rn(wzy, wx[xx]);
-              acc[xx].x = __fmaf_rn(wt, v.x, acc[xx].x);
-              acc[xx].y = __fmaf_rn(wt, v.y, acc[xx].y);
-            }
-#pragma unroll
-          for (int xx = 0; xx < KS; ++xx)
-            if (xx < nx)
-              trow[(size_t)lx[xx] * PITCH] = acc[xx];
-        }
-      }
-    }
-  }
-  __syncthreads();
-
-  // store the owned cells of each coil of the group: per-CTA offset tables
-  // (shifted, clipped rows and columns), then division-free loops with
-  // lanes along x
-  const long long G = g.grid_count;
-  const int nrows = DIM == 3 ? sw * sw : sw;
-  long long *s_rowoff = reinterpret_cast<long long *>(s_v);  // reuse
-  int *s_xoff = reinterpret_cast<int *>(s_rowoff + nrows);
-  for (int r = threadIdx.x; r < nrows; r += nthreads)
-  {
-    const int y = r % sw, z = DIM == 3 ? r / sw : 0;
-    int gy = ta[1] * sw + y, gz = DIM == 3 ? ta[2] * sw + z : 0;
-    long long off = -1;
-    if (gy < g.G[1] && gz < g.G[2])
-    {
-      if (shift)
-      {
-        gy = wrap_mod(gy - g.shift_inv[1], g.G[1]);
-        gz = DIM == 3 ? wrap_mod(gz - g.shift_inv[2], g.G[2]) : 0;
-      }
-      off = ((long long)gz * g.G[1] + gy) * g.G[0];
-    }
-    s_rowoff[r] = off;
-  }
-  for (int x = threadIdx.x; x < sw; x += nthreads)
-  {
-    const int gx = ta[0] * sw + x;
-    int off = -1;
-    if (gx < g.G[0])
-      off = shift ? wrap_mod(gx - g.shift_inv[0], g.G[0]) : gx;
-    s_xoff[x] = off;
-  }
-  __syncthreads();
-  {
-    const int lanes_per_row = sw < 32 ? sw : 32;
-    const int x0 = threadIdx.x % lanes_per_row;
-    const int rstep = nthreads / lanes_per_row;
-    const int r0 = threadIdx.x / lanes_per_row;
-    if (r0 < rstep)
-    {
-      for (int cl = 0; cl < CG; ++cl)
-      {
-        const int c = group * CG + cl;
-        if (c >= C)
-          break;
-        float2 *gc = grid + (long long)c * G;
-        for (int r = r0; r < nrows; r += rstep)
-        {
-          const long long ro = s_rowoff[r];
-          if (ro < 0)
-            continue;
-          for (int x = x0; x < sw; x += lanes_per_row)
-          {
-            const int xo = s_xoff[x];
-            if (xo < 0)
-              continue;
-            const float2 v = tile[(size_t)(r * sw + x) * PITCH + cl];
-            if (it.split)
-            {
-              atomicAdd(&gc[ro + xo].x, v.x);
-              atomicAdd(&gc[ro + xo].y, v.y);
-            }
-            else
-            {
-              gc[ro + xo] = v;
-            }
-          }
-        }
-      }
-    }
-  }
-}
-
-// Zero the owned cells of targets that no spread block writes with plain
-// stores (targets without candidates, and split targets whose blocks add
-// atomically).  One block per target; lanes along x, no divisions per cell.
-template <int DIM>
-__global__ void k_zero_targets(const int *__restrict__ targets, Geo g, int C,
-                               int shift, float2 *__restrict__ grid)
-{
-  __shared__ long long s_rowoff[kMaxBuckets * kMaxBuckets];
-  __shared__ int s_xoff[kMaxBuckets];
-  int ta[3];
-  split_sector(targets[blockIdx.x], g, ta);
-  const int sw = g.sw;
-  const int nrows = DIM == 3 ? sw * sw : sw;
-  for (int r = threadIdx.x; r < nrows; r += blockDim.x)
-  {
-    const int y = r % sw, z = DIM == 3 ? r / sw : 0;
-    int gy = ta[1] * sw + y, gz = DIM == 3 ? ta[2] * sw + z : 0;
-    long long off = -1;
-    if (gy < g.G[1] && gz < g.G[2])
-    {
-      if (shift)
-      {
-        gy = wrap_mod(gy - g.shift_inv[1], g.G[1]);
-        gz = DIM == 3 ? wrap_mod(gz - g.shift_inv[2], g.G[2]) : 0;
-      }
-      off = ((long long)gz * g.G[1] + gy) * g.G[0];
-    }
-    s_rowoff[r] = off;
-  }
-  for (int x = threadIdx.x; x < sw; x += blockDim.x)
-  {
-    const int gx = ta[0] * sw + x;
-    s_xoff[x] = gx < g.G[0] ? (shift ? wrap_mod(gx - g.shift_inv[0], g.G[0])
-                                     : gx)
-                            : -1;
-  }
-  __syncthreads();
-  const int x0 = threadIdx.x % sw;
-  const int rstep = blockDim.x / sw;
-  const int r0 = threadIdx.x / sw;
-  if (r0 >= rstep)
-    return;
-  const int xo = s_xoff[x0];
-  if (xo < 0)
-    return;
-  for (int c = 0; c < C; ++c)
-  {
-    float2 *gc = grid + (long long)c * g.grid_count + xo;
-    for (int r = r0; r < nrows; r += rstep)
-    {
-      const long long ro = s_rowoff[r];
-      if (ro >= 0)
-        gc[ro] = make_float2(0.f, 0.f);
-    }
-  }
-}
+// Sector widths above this are rejected (plan-time tables and tiles are
+// sized for it).
+constexpr int kMaxSectorWidth = 32;
 
 // --------------------------------------------------------------------------
 // adjoint as a product with the interpolation matrix (CSR by grid cell)
@@ -1144,8 +772,8 @@ __global__ void __launch_bounds__(kThreads)
         float w[KS];
         int nn = 0;
         if (t < it.end)
-          nn = compact_axis<KS>(traj[(size_t)a * M + t], a, sa[a], 0, g, lut,
-                                false, l, w);
+          nn = compact_axis<KS>(traj[(size_t)a * M + t], a, sa[a], g, lut, l,
+                                w);
         // tile frame: entries are consecutive cells starting at l[0]
         s_b[a * CH + threadIdx.x] = (nn ? l[0] : 0) | (nn << 16);
 #pragma unroll
@@ -1345,8 +973,8 @@ __global__ void __launch_bounds__(kThreads)
     w[2][0] = 1.f;
 #pragma unroll
     for (int a = 0; a < DIM; ++a)
-      n[a] = compact_axis<KS>(__ldg(traj + (size_t)a * M + t), a, sa[a], 0, g,
-                              lut, false, l[a], w[a]);
+      n[a] = compact_axis<KS>(__ldg(traj + (size_t)a * M + t), a, sa[a], g,
+                              lut, l[a], w[a]);
     float2 acc[CG];
 #pragma unroll
     for (int c = 0; c < CG; ++c)
@@ -1495,7 +1123,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
       n[s][a] = 0;
       if (t < it.end)
         n[s][a] = compact_axis<KS>(__ldg(traj + (size_t)a * M + t), a, sa[a],
-                                   0, g, lut, false, l, w[s][a]);
+                                   g, lut, l, w[s][a]);
       else
       {
 #pragma unroll
@@ -1822,25 +1450,6 @@ void set_smem(K kernel, size_t bytes)
 }
 
 template <int DIM, int CG, int KS>
-void adj_dispatch(const AdjItem *items, int n_items, const uint32_t *cand,
-                  const uint32_t *sector_sorted, const float *traj,
-                  const float2 *ks, int CP, const Geo &g, const float *lut,
-                  uint32_t M, int C, bool shift, float2 *grid, cudaStream_t s)
-{
-  const int threads = adjoint_block_threads(g, CG);
-  int ch = threads < 128 ? threads : 128;
-  while (ch > 32 && adjoint_smem_bytes(g, CG, ch) > 110 * 1024)
-    ch >>= 1;
-  const size_t smem = adjoint_smem_bytes(g, CG, ch);
-  auto k = k_adjoint_spread<DIM, CG, KS>;
-  set_smem(k, smem);
-  dim3 grd(n_items, (C + CG - 1) / CG);
-  k<<<grd, threads, smem, s>>>(items, cand, sector_sorted, traj, ks, CP, g,
-                               lut, M, C, shift ? 1 : 0, ch, grid);
-  GN_LAUNCH_CHECK("adjoint spread");
-}
-
-template <int DIM, int CG, int KS>
 void fwd_dispatch(const FwdItem *items, int n_items, const float *traj,
                   const uint32_t *idx, const float *dens, const float2 *grid,
                   const Geo &g, const float *lut, uint32_t M, int C,
@@ -1867,28 +1476,16 @@ int pow2_at_least(int c)
 int slots_for(const Geo &g) { return g.kw + 1 <= 4 ? 4 : 8; }
 }  // namespace
 
-// 16 coil lanes per group for larger coil counts: two resident blocks per
-// SM (the 32-lane tile alone takes ~135 KB of shared memory in 3-D); fewer
-// lanes when the sector tile is large.
-int adjoint_coil_group(int C, const Geo &g)
-{
-  int cg = C > 8 ? 16 : pow2_at_least(C);
-  while (cg > 1 && adjoint_smem_bytes(g, cg, 32) > 200 * 1024)
-    cg >>= 1;
-  return cg;
-}
-
 int spmm_coil_group(int C) { return C > 16 ? 32 : pow2_at_least(C); }
 
 bool gridding_supported(const Geo &g, std::string &why)
 {
-  if (g.sw > kMaxBuckets)
+  if (g.sw > kMaxSectorWidth)
   {
     why = "sector width above 32 is not supported";
     return false;
   }
-  if (adjoint_smem_bytes(g, 1, 32) > 200 * 1024 ||
-      forward_smem_bytes(g, 1) > 200 * 1024)
+  if (forward_smem_bytes(g, 1) > 200 * 1024)
   {
     why = "sector tile exceeds shared memory (3-D sector width too large)";
     return false;
@@ -1906,30 +1503,6 @@ int forward_coil_group(int C, int dim, int pad)
   if (dim == 2)
     cg = C > 16 ? 32 : pow2_at_least(C);
   return cg;
-}
-
-// One unit (warp slot) per owned plane of the target: sw planes.
-int adjoint_block_threads(const Geo &g, int cg)
-{
-  const int slots = 32 / cg;
-  int warps = (g.sw + slots - 1) / slots;
-  warps = warps < 1 ? 1 : (warps > 16 ? 16 : warps);
-  return 32 * warps;
-}
-
-size_t adjoint_smem_bytes(const Geo &g, int cg, int threads)
-{
-  // `threads` = candidates per chunk (CH); per-warp counters sized for 16
-  const size_t cells = g.dim == 3 ? (size_t)g.sw * g.sw * g.sw
-                                  : (size_t)g.sw * g.sw;
-  const int ks = g.kw + 1 <= 4 ? 4 : 8;
-  const int nb = g.sw < 32 ? g.sw : 32;
-  return cells * (cg + 1) * sizeof(float2) +
-         (size_t)threads * (1 + g.dim + 2 * g.dim * ks) * 4 +
-         ((size_t)nb * threads + 1) / 2 * 4 + 4 + (size_t)nb * 17 * 4 + 16 +
-         std::max((size_t)threads * cg * sizeof(float2),
-                  (size_t)(g.dim == 3 ? g.sw * g.sw : g.sw) * 8 +
-                      (size_t)g.sw * 4);
 }
 
 size_t forward_smem_bytes(const Geo &g, int cg)
@@ -1954,59 +1527,6 @@ void launch_gather_kspace(const float2 *kspace, const uint32_t *idx,
   GN_LAUNCH_CHECK("gather k-space");
 }
 
-void launch_zero_split(const int *targets, int n_targets, const Geo &g, int C,
-                       bool shift, float2 *grid, cudaStream_t s)
-{
-  if (n_targets <= 0)
-    return;
-  if (g.sw > kMaxBuckets)
-    throw Error(kNotSupported, "sector width above 32");
-  if (g.dim == 3)
-    k_zero_targets<3><<<n_targets, kThreads, 0, s>>>(targets, g, C, shift,
-                                                     grid);
-  else
-    k_zero_targets<2><<<n_targets, kThreads, 0, s>>>(targets, g, C, shift,
-                                                     grid);
-  GN_LAUNCH_CHECK("zero targets");
-}
-
-void launch_adjoint_spread(const AdjItem *items, int n_items,
-                           const uint32_t *cand, const uint32_t *sector_sorted,
-                           const float *traj_sorted, const float2 *ks, int CP,
-                           const Geo &g, const float *lut, uint32_t M, int C,
-                           bool shift, float2 *grid, cudaStream_t s)
-{
-  if (n_items <= 0)
-    return;
-  const int cg = adjoint_coil_group(C, g);
-#define GN_ADJ(D, CGV)                                                         \
-  if (slots_for(g) == 4)                                                       \
-    adj_dispatch<D, CGV, 4>(items, n_items, cand, sector_sorted, traj_sorted, \
-                            ks, CP, g, lut, M, C, shift, grid, s);            \
-  else                                                                         \
-    adj_dispatch<D, CGV, 8>(items, n_items, cand, sector_sorted, traj_sorted, \
-                            ks, CP, g, lut, M, C, shift, grid, s)
-#define GN_ADJ_CG(D)                                                           \
-  switch (cg)                                                                  \
-  {                                                                            \
-  case 1: GN_ADJ(D, 1); break;                                                 \
-  case 2: GN_ADJ(D, 2); break;                                                 \
-  case 4: GN_ADJ(D, 4); break;                                                 \
-  case 8: GN_ADJ(D, 8); break;                                                 \
-  case 16: GN_ADJ(D, 16); break;                                               \
-  default: GN_ADJ(D, 32); break;                                               \
-  }
-  if (g.dim == 3)
-  {
-    GN_ADJ_CG(3)
-  }
-  else
-  {
-    GN_ADJ_CG(2)
-  }
-#undef GN_ADJ_CG
-#undef GN_ADJ
-}
 
 void launch_adjoint_spmm(const uint32_t *row_off, const uint2 *nz,
                          const float2 *ks, int CP, const Geo &g, int C,

@@ -11,17 +11,6 @@
 namespace gnufft
 {
 
-// Adjoint work item: one owner sector (target) and a slice of its candidate
-// list.  `split` != 0 when the target's candidates are spread over several
-// items; those accumulate into the (pre-zeroed) grid with atomics.
-struct AdjItem
-{
-  int target;
-  int begin;
-  int end;
-  int split;
-};
-
 // Forward work item: samples [begin, end) of one sector, at most
 // kFwdItemSamples of them.
 constexpr int kFwdItemSamples = 512;
@@ -33,15 +22,11 @@ struct FwdItem
   int pad_;
 };
 
-// Coil-group width used by the spread / interpolation kernels for C coils.
-int adjoint_coil_group(int C, const Geo &g);
 // Whether the sector tiles of this geometry fit the kernels (why if not).
 bool gridding_supported(const Geo &g, std::string &why);
+// Coil-group width of the forward interpolation for C coils.
 int forward_coil_group(int C, int dim, int pad);
-
-// Launch shape / dynamic shared memory of the kernels.
-int adjoint_block_threads(const Geo &g, int cg);
-size_t adjoint_smem_bytes(const Geo &g, int cg, int chunk);
+// Dynamic shared memory of the forward interpolation (general grids).
 size_t forward_smem_bytes(const Geo &g, int cg);
 
 // ks[t*CP + c] = kspace[c*M + idx[t]] * sqrt(dens[t]) (dens may be NULL);
@@ -50,19 +35,6 @@ size_t forward_smem_bytes(const Geo &g, int cg);
 void launch_gather_kspace(const float2 *kspace, const uint32_t *idx,
                           const float *dens_sorted, uint32_t M, int C, int CP,
                           float2 *ks, cudaStream_t s);
-
-// Zero the owned cells of the split targets in grid [C][G].
-void launch_zero_split(const int *targets, int n_targets, const Geo &g, int C,
-                       bool shift, float2 *grid, cudaStream_t s);
-
-// Adjoint spread: every target writes its owned cells of grid [C][G] once.
-// With `shift`, cell g is stored at (g - floor(G/2)) mod G per axis (the
-// upstream's INVERSE fftshift ahead of the inverse FFT).
-void launch_adjoint_spread(const AdjItem *items, int n_items,
-                           const uint32_t *cand, const uint32_t *sector_sorted,
-                           const float *traj_sorted, const float2 *ks, int CP,
-                           const Geo &g, const float *lut, uint32_t M, int C,
-                           bool shift, float2 *grid, cudaStream_t s);
 
 // Coil-group width of the sparse adjoint (lanes per cell).
 int spmm_coil_group(int C);

@@ -40,8 +40,7 @@ namespace
 {
 thread_local std::string g_last_error;
 
-// Candidates per adjoint work item and samples per forward work item.
-constexpr int kAdjPayload = 2048;
+// Samples per forward work item.
 constexpr int kFwdPayload = kFwdItemSamples;
 
 // Mirrors the upstream IndPair (gpuNUFFT_types.hpp:33-49): compared by the
@@ -83,16 +82,15 @@ struct gnufft_plan
   bool has_dens = false;
 
   // resident device tables
-  DeviceBuffer lut, traj_sorted, di, sec_sorted, dens_sorted, cand, cand_off;
-  DeviceBuffer adj_items, split_targets, fwd_items, deapo, sens;
+  DeviceBuffer lut, traj_sorted, di, sec_sorted, dens_sorted;
+  DeviceBuffer fwd_items, deapo, sens;
   DeviceBuffer w_rows, w_nz;  // interpolation matrix, CSR by grid cell
   DeviceBuffer dlut;          // kernel derivative table (trajectory gradient)
   DeviceBuffer roots[3];      // DFT roots per axis (pruned transforms)
   DeviceBuffer zrange;        // per (y, x) column: z rows with weights
   float dlut_mult = 0.f;
   size_t nnz = 0;
-  int n_adj_items = 0, n_split = 0, n_fwd_items = 0;
-  size_t n_cand = 0;
+  int n_fwd_items = 0;
   uint32_t sens_coils = 0;
   std::vector<float2> sens_h;
 
@@ -129,8 +127,7 @@ struct gnufft_plan
   size_t device_bytes() const
   {
     const DeviceBuffer *bufs[] = {&lut,         &traj_sorted, &di,
-                                  &sec_sorted,  &dens_sorted, &cand,
-                                  &cand_off,    &adj_items,   &split_targets,
+                                  &sec_sorted,  &dens_sorted,
                                   &fwd_items,   &deapo,       &sens,
                                   &w_rows,      &w_nz,
                                   &ks,          &grid,        &stage_in,

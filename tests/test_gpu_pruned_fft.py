@@ -23,6 +23,11 @@ CASES = [
     ((16, 32, 8), lambda r: r.uniform(-0.5, 0.5, (3, 3000)), 3, 2.0, 3),
     ((32, 32, 32), lambda r: kooshball_3d(500, 64), 33, 2.0, 3),
     ((64, 64, 64), lambda r: kooshball_3d(800, 128), 2, 2.0, 5),
+    # odd image widths on power-of-two grids (15 * 2.1334 -> 32): odd
+    # crop offsets, and column passes over N_x = 15 columns (no tensor
+    # copies: rows of odd length are not 16-byte strided)
+    ((15, 30), lambda r: radial_2d(40, 64), 3, 2.1334, 3),
+    ((15, 15, 15), lambda r: kooshball_3d(300, 32), 20, 2.1334, 3),
 ]
 
 
