@@ -152,14 +152,22 @@ class PlanCache:
 
 
 class _Active:
-    """A request on the GPU: its plan instance, stream and CG state."""
+    """A request on the GPU: its plan instance, stream and CG state.
 
-    def __init__(self, req: Request, plan: Plan, device: int):
+    The CG vectors live in fixed device tensors updated in place, so after
+    the first (eager) iteration one iteration is captured as a CUDA graph
+    and every later iteration is a single graph launch: the host work per
+    iteration no longer grows with the number of kernels in it."""
+
+    def __init__(self, req: Request, plan: Plan, device: int,
+                 use_graph: bool = True):
         self.req = req
         self.plan = plan
         self.stream = torch.cuda.Stream(device=device)
         self.done_event = torch.cuda.Event()
         self.it = 0
+        self.use_graph = use_graph
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
         with torch.cuda.stream(self.stream):
             dev = torch.device("cuda", device)
             # pinned host tensors upload asynchronously on this stream
@@ -172,18 +180,40 @@ class _Active:
             self.p = rhs.clone()
             self.rr = _dot(self.r, self.r).real
 
+    def _iteration(self) -> None:
+        """One CG iteration (matlab/demo/utils/cg_sense_2d.m:76-100) with
+        in-place updates of x, r, p and rr."""
+        ap = self.plan.adjoint(self.plan.forward(self.p))
+        if self.req.alpha:
+            ap = ap + self.req.alpha * self.p
+        a = self.rr / _dot(self.p, ap)
+        self.x.add_(a * self.p)
+        self.r.sub_(a * ap)
+        rr_new = _dot(self.r, self.r).real
+        self.p.mul_(rr_new / self.rr).add_(self.r)
+        self.rr.copy_(rr_new)
+
     def step(self) -> None:
         """Enqueue one CG iteration on this request's stream."""
         with torch.cuda.stream(self.stream):
-            ap = self.plan.adjoint(self.plan.forward(self.p))
-            if self.req.alpha:
-                ap = ap + self.req.alpha * self.p
-            a = self.rr / _dot(self.p, ap)
-            self.x = self.x + a * self.p
-            self.r = self.r - a * ap
-            rr_new = _dot(self.r, self.r).real
-            self.p = self.r + (rr_new / self.rr) * self.p
-            self.rr = rr_new
+            if self.graph is not None:
+                self.graph.replay()
+            elif self.use_graph and self.it == 1 and self.req.n_iter > 2:
+                # the first iteration ran eagerly on this stream (every
+                # buffer of the plan and of the vector ops exists); capture
+                # the second and replay it from now on.  capture_begin /
+                # capture_end, not torch.cuda.graph: no device-wide
+                # synchronisation while other requests run.
+                g = torch.cuda.CUDAGraph()
+                g.capture_begin()
+                try:
+                    self._iteration()
+                finally:
+                    g.capture_end()
+                self.graph = g
+                g.replay()
+            else:
+                self._iteration()
             self.it += 1
             if self.it == self.req.n_iter:
                 self.out = torch.empty(self.x.shape, dtype=self.x.dtype,
@@ -193,6 +223,9 @@ class _Active:
 
     def finished(self) -> bool:
         return self.it == self.req.n_iter and self.done_event.query()
+
+    def release(self) -> None:
+        self.graph = None
 
 
 class Server:
@@ -263,6 +296,7 @@ class Server:
             if a.finished():
                 a.req.result = a.out.numpy().copy()
                 a.req.finished = self.now()
+                a.release()
                 self.cache.release(a.plan)
                 self.in_use -= estimate_bytes(a.req)
                 self.done.append(a.req)
@@ -322,6 +356,7 @@ class Server:
     def close(self) -> None:
         torch.cuda.synchronize(self.device)
         for a in self.active:
+            a.release()
             self.cache.release(a.plan)
         self.active = []
         self.cache.clear()
