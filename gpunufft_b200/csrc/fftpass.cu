@@ -399,7 +399,7 @@ __global__ void k_sum_coil_groups(const float2 *__restrict__ partial,
 // rows, so the image is read once per block.  Output A[c][row][k],
 // rows = N_y * N_z.
 template <int L, bool SENS>
-__global__ void __launch_bounds__(kFftThreads, L <= 256 ? 3 : 1)
+__global__ void __launch_bounds__(kFftThreads, L <= 256 ? 4 : 1)
     k_fft_rows_fwd(const float2 *__restrict__ image,
                    const float2 *__restrict__ sens,
                    const float *__restrict__ deapo, int Nx, long long rows,
