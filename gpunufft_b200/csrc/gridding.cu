@@ -224,8 +224,11 @@ __device__ __forceinline__ int acc_pos(int cell, int c)
 // entry (after a barrier); acc holds every cell after the caller's next
 // barrier.  A unit whose last cell continues in the next shares leaves its
 // partial sum in acc; the following units' partials (part_head) are added
-// to it in unit order.
-template <int CG, int V, int SR2 = 0>
+// to it in unit order.  With ZG the caller zeroes only the empty cells
+// before the row's first and after its last nonzero: every unit stores
+// each cell it passes (zero sums included), and the empty cells between
+// two units' cells are zeroed by the later unit.
+template <int CG, int V, int SR2 = 0, bool ZG = false>
 __device__ __forceinline__ void spmm_accumulate(
     const uint32_t *s_off, int nxc, const uint2 *__restrict__ nz,
     const float2 *__restrict__ ks, int CP, int group, float2 *acc,
@@ -253,6 +256,13 @@ __device__ __forceinline__ void spmm_accumulate(
     const int i = base + cl + 1;
     const bool le = i <= nxc && s_off[i] <= u0;
     cell += __popc(__ballot_sync(0xffffffffu, le) & slot_bits);
+  }
+  if (ZG && A < u0 && u0 < u1)
+  {  // empty cells just before this unit's first cell start at u0
+    for (int c = cell - 1; c >= 0 && s_off[c] == u0; --c)
+#pragma unroll
+      for (int v = 0; v < V; ++v)
+        acc[acc_pos<CG, SR2>(c, cl * V + v)] = make_float2(0.f, 0.f);
   }
   if (u0 < u1)
   {
@@ -492,7 +502,7 @@ template <int CG, int L> struct XfftLayout
   static size_t scratch(int NU)
   {
     return (size_t)NU * CG * sizeof(float2) + (size_t)(L + 1) * 4 +
-           (size_t)2 * NU * 4;
+           (size_t)(2 * NU + 2) * 4;
   }
   static size_t smem(int NU)
   {
@@ -551,16 +561,32 @@ __global__ void __launch_bounds__(kThreads, L <= 256 ? 3 : 1)
     }
     return;
   }
+  // only the empty cells before the row's first and after its last nonzero
+  // need zeros (the spread stores every other cell): find both ends, then
+  // zero those whole cells (contiguous in either layout)
+  int *s_ends = tail_cell + NU;
+  for (int i = threadIdx.x; i < L; i += kThreads)
   {
-    float4 *a4 = reinterpret_cast<float4 *>(acc);
-    for (int i = threadIdx.x; i < Lay::ACC / 2; i += kThreads)
-      a4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t a = s_off[i], b = s_off[i + 1];
+    if (a == s_off[0] && b > a)
+      s_ends[0] = i;
+    if (a < b && b == s_off[L])
+      s_ends[1] = i;
   }
   for (int i = threadIdx.x; i < NU; i += kThreads)
     head_cell[i] = tail_cell[i] = -1;
   __syncthreads();
-  spmm_accumulate<CG, V, SR2>(s_off, L, nz, ks, CP, group, acc, part_head,
-                              head_cell, tail_cell);
+  {
+    constexpr int PITCH = IP ? CG : CG + 1;  // float2 per cell
+    float2 *lo_end = acc + (size_t)s_ends[0] * PITCH;
+    for (float2 *q = acc + threadIdx.x; q < lo_end; q += kThreads)
+      *q = make_float2(0.f, 0.f);
+    for (float2 *q = acc + (size_t)(s_ends[1] + 1) * PITCH + threadIdx.x;
+         q < acc + (size_t)L * PITCH; q += kThreads)
+      *q = make_float2(0.f, 0.f);
+  }
+  spmm_accumulate<CG, V, SR2, true>(s_off, L, nz, ks, CP, group, acc,
+                                    part_head, head_cell, tail_cell);
   __syncthreads();
 
   // inverse DFT along x of each coil's row, NL coils per pass
