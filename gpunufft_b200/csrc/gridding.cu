@@ -113,6 +113,63 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// The same gather driven by the original order: a block reads 64
+// consecutive original samples of 32 coils (coalesced per coil), and writes
+// each sample's coil row (contiguous) to its sorted position inv[j].
+__global__ void __launch_bounds__(kThreads)
+    k_gather_kspace_inv(const float2 *__restrict__ kspace,
+                        const uint32_t *__restrict__ inv,
+                        const float *__restrict__ dens, uint32_t M, int C,
+                        int CP, float2 *__restrict__ ks)
+{
+  __shared__ float2 tile[kGatherSamples][kGatherCoils + 1];
+  __shared__ uint32_t s_t[kGatherSamples];
+  __shared__ float sd[kGatherSamples];
+  const size_t j0 = (size_t)blockIdx.x * kGatherSamples;
+  const int c0 = blockIdx.y * kGatherCoils;
+  const int nc = min(kGatherCoils, CP - c0);
+  for (int i = threadIdx.x; i < kGatherSamples; i += kThreads)
+  {
+    const size_t j = j0 + i;
+    const uint32_t t = j < M ? __ldg(inv + j) : 0u;
+    s_t[i] = t;
+    sd[i] = (dens && j < M) ? sqrtf(__ldg(dens + t)) : 1.0f;
+  }
+  for (int i = threadIdx.x; i < kGatherSamples * nc; i += kThreads)
+  {
+    const int jl = i % kGatherSamples, cl = i / kGatherSamples;
+    const size_t j = j0 + jl;
+    const int c = c0 + cl;
+    float2 v = make_float2(0.f, 0.f);
+    if (j < M && c < C)
+      v = __ldg(kspace + (size_t)c * M + j);
+    tile[jl][cl] = v;
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < kGatherSamples * nc; i += kThreads)
+  {
+    const int cl = i % nc, jl = i / nc;
+    if (j0 + jl < M)
+    {
+      float2 v = tile[jl][cl];
+      if (dens)
+      {  // density compensation: x * sqrt(w) per component
+        v.x = __fmul_rn(v.x, sd[jl]);
+        v.y = __fmul_rn(v.y, sd[jl]);
+      }
+      ks[(size_t)s_t[jl] * CP + c0 + cl] = v;
+    }
+  }
+}
+
+__global__ void k_invert(const uint32_t *__restrict__ idx, uint32_t M,
+                         uint32_t *__restrict__ inv)
+{
+  for (size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x; t < M;
+       t += (size_t)gridDim.x * blockDim.x)
+    inv[idx[t]] = (uint32_t)t;
+}
+
 // --------------------------------------------------------------------------
 // compact per-axis footprints (phase A: one sample per thread)
 // --------------------------------------------------------------------------
@@ -1538,6 +1595,28 @@ size_t forward_smem_bytes(const Geo &g, int cg)
   const int ks = g.kw + 1 <= 4 ? 4 : 8;
   return cells * (cg + 1) * sizeof(float2) +
          (size_t)kThreads * (g.dim + g.dim * ks) * 4 + 8 + (size_t)g.pad * 16;
+}
+
+void launch_gather_kspace_inv(const float2 *kspace, const uint32_t *inv,
+                              const float *dens_sorted, uint32_t M, int C,
+                              int CP, float2 *ks, cudaStream_t s)
+{
+  if (!M)
+    return;
+  dim3 grd((M + kGatherSamples - 1) / kGatherSamples,
+           (CP + kGatherCoils - 1) / kGatherCoils);
+  k_gather_kspace_inv<<<grd, kThreads, 0, s>>>(kspace, inv, dens_sorted, M,
+                                               C, CP, ks);
+  GN_LAUNCH_CHECK("gather k-space (original order)");
+}
+
+void launch_invert_permutation(const uint32_t *idx, uint32_t M,
+                               uint32_t *inv, cudaStream_t s)
+{
+  if (!M)
+    return;
+  k_invert<<<grid_for(M, 256, 8192), 256, 0, s>>>(idx, M, inv);
+  GN_LAUNCH_CHECK("invert permutation");
 }
 
 void launch_gather_kspace(const float2 *kspace, const uint32_t *idx,

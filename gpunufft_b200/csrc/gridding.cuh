@@ -35,6 +35,15 @@ size_t forward_smem_bytes(const Geo &g, int cg);
 void launch_gather_kspace(const float2 *kspace, const uint32_t *idx,
                           const float *dens_sorted, uint32_t M, int C, int CP,
                           float2 *ks, cudaStream_t s);
+// The same result, reading the k-space in its original order (coalesced)
+// and writing each sample's coil row to its sorted position inv[j]
+// (inv = the inverse of the data-index permutation).
+void launch_gather_kspace_inv(const float2 *kspace, const uint32_t *inv,
+                              const float *dens_sorted, uint32_t M, int C,
+                              int CP, float2 *ks, cudaStream_t s);
+// inv[idx[t]] = t.
+void launch_invert_permutation(const uint32_t *idx, uint32_t M,
+                               uint32_t *inv, cudaStream_t s);
 
 // Coil-group width of the sparse adjoint (lanes per cell).
 int spmm_coil_group(int C);

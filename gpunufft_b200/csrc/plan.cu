@@ -84,6 +84,7 @@ struct gnufft_plan
   // resident device tables
   DeviceBuffer lut, traj_sorted, di, sec_sorted, dens_sorted;
   DeviceBuffer fwd_items, deapo, sens;
+  DeviceBuffer di_inv;  // sorted position of every original sample
   DeviceBuffer w_rows, w_nz;  // interpolation matrix, CSR by grid cell
   DeviceBuffer dlut;          // kernel derivative table (trajectory gradient)
   DeviceBuffer roots[3];      // DFT roots per axis (pruned transforms)
@@ -129,6 +130,7 @@ struct gnufft_plan
     const DeviceBuffer *bufs[] = {&lut,         &traj_sorted, &di,
                                   &sec_sorted,  &dens_sorted,
                                   &fwd_items,   &deapo,       &sens,
+                                  &di_inv,
                                   &w_rows,      &w_nz,
                                   &ks,          &grid,        &stage_in,
                                   &stage_out,   &one_sens,    &fft_a,
@@ -376,6 +378,9 @@ void finish_tables(gnufft_plan &p)
                               p.sec_sorted.as<uint32_t>(), p.M, p.g,
                               p.lut.as<float>(), p.w_rows, p.w_nz, p.stream);
   build_items(p);
+  p.di_inv.reset((size_t)p.M * sizeof(uint32_t) + 4);
+  launch_invert_permutation(p.di.as<uint32_t>(), p.M, p.di_inv.as<uint32_t>(),
+                            p.stream);
   if (p.pruned && p.dim == 3)
     build_column_ranges(p.w_rows.as<uint32_t>(), p.g, p.zrange, p.stream);
   processing_order(p.sdc_h, p.order_h);
@@ -597,9 +602,9 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
     grid = p.grid.as<float2>();
   }
   p.mark(0, s);
-  launch_gather_kspace(k, p.di.as<uint32_t>(),
-                       p.has_dens ? p.dens_sorted.as<float>() : nullptr, p.M,
-                       (int)C, CP, p.ks.as<float2>(), s);
+  launch_gather_kspace_inv(k, p.di_inv.as<uint32_t>(),
+                           p.has_dens ? p.dens_sorted.as<float>() : nullptr,
+                           p.M, (int)C, CP, p.ks.as<float2>(), s);
   p.launches += 1;
   p.mark(1, s);
   p.mark(2, s);
