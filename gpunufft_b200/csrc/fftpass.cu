@@ -170,7 +170,41 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
   }
 }
 
-template <int L, bool INV>
+// Tile t of a pass over `planes` planes of n_ct column tiles.  PAIRED:
+// the two planes (coils) of a pair take adjacent tiles (t, t + 1 ->
+// planes 2p, 2p + 1 of the same columns, so that the two halves of every
+// interleaved output pair are written close in time); an odd last plane
+// follows on its own.
+template <bool PAIRED>
+__device__ __forceinline__ void col_tile_of(long long t, long long n_ct,
+                                            long long planes, long long &plane,
+                                            long long &ct)
+{
+  if (!PAIRED)
+  {
+    plane = t / n_ct;
+    ct = t - plane * n_ct;
+    return;
+  }
+  const long long paired = n_ct * (planes & ~1LL);
+  if (t < paired)
+  {
+    const long long pr = t / (2 * n_ct), rem = t - pr * 2 * n_ct;
+    ct = rem >> 1;
+    plane = 2 * pr + (rem & 1);
+  }
+  else
+  {
+    plane = planes - 1;
+    ct = t - paired;
+  }
+}
+
+// PAIRED: output element (plane c, row r, column col) at
+// ((c / 2) * dst_rows * ncols + r * ncols + col) * 2 + c % 2, i.e. coil
+// pairs interleaved (the layout the 3-D forward interpolation reads two
+// coils of a cell from with one 16-byte load).
+template <int L, bool INV, bool PAIRED>
 __global__ void __launch_bounds__(Shape<L>::CT, 3)
     k_fft_cols_tma(const __grid_constant__ CUtensorMap tmap,
                    float2 *__restrict__ dst, long long ncols, long long n_ct,
@@ -191,11 +225,13 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
   const uint32_t buf0 = tma::smem_addr(buf);
   const uint32_t bytes = (uint32_t)(ncopy * box_rows) * 128u;
   const long long stride = gridDim.x;
+  const long long planes = n_tiles / n_ct;
   auto issue = [&](long long t, int b) {
-    const long long plane = t / n_ct;
+    long long plane, ct;
+    col_tile_of<PAIRED>(t, n_ct, planes, plane, ct);
     col_tile_issue(&tmap, buf0 + (uint32_t)b * (uint32_t)T::tile_bytes,
-                   bar0 + 8u * (uint32_t)b, (int)(t - plane * n_ct) * TC,
-                   (int)plane, box_rows, ncopy, bytes);
+                   bar0 + 8u * (uint32_t)b, (int)ct * TC, (int)plane,
+                   box_rows, ncopy, bytes);
   };
   if (threadIdx.x == 0)
   {
@@ -234,8 +270,9 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
       }
       return;
     }
-    const long long plane = t / n_ct;
-    const long long col = (t - plane * n_ct) * TC + cl;
+    long long plane, ct;
+    col_tile_of<PAIRED>(t, n_ct, planes, plane, ct);
+    const long long col = ct * TC + cl;
     uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
     if (colrange && col < ncols)
       cr = __ldg(colrange + col);
@@ -245,13 +282,16 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
                          w, tw, bv);
     if (lt < S::R1 && on)
     {
-      float2 *dp = dst + plane * dst_rows * ncols + col;
+      const long long psz = (long long)dst_rows * ncols;
+      float2 *dp = PAIRED ? dst + ((plane >> 1) * psz + col) * 2 + (plane & 1)
+                          : dst + plane * psz + col;
+      const long long rs = PAIRED ? 2 * ncols : ncols;
 #pragma unroll
       for (int k2 = 0; k2 < S::R2; ++k2)
       {
         const int r = (lt + S::R1 * k2 + out_add) & (L - 1);
         if (r < out_count && (unsigned)r >= cr.x && (unsigned)r <= cr.y)
-          dp[(long long)r * ncols] = bv[k2];
+          dp[(long long)r * rs] = bv[k2];
       }
     }
     tma::fence_proxy_async();  // the in-place writes before the refill
@@ -702,7 +742,8 @@ template <bool INV>
 void cols(int L, const float2 *src, float2 *dst, long long ncols,
           int src_rows, int dst_rows, long long planes, int in_add,
           int in_count, int out_add, int out_count, const float2 *roots,
-          cudaStream_t s, const uint2 *colrange = nullptr, int *err = nullptr)
+          cudaStream_t s, const uint2 *colrange = nullptr, int *err = nullptr,
+          bool paired = false)
 {
   bool done = false;
   if (err && L <= 256)
@@ -720,17 +761,24 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
           return;
         const long long n_ct = (ncols + S::TC - 1) / S::TC;
         const long long n_tiles = n_ct * planes;
-        auto k = k_fft_cols_tma<LL, INV>;
-        set_smem(k, ColTma<LL>::smem());
-        k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
-            tm, dst, ncols, n_ct, n_tiles, box_rows, ncopy, dst_rows, in_add,
-            in_count, out_add, out_count, roots, colrange, err);
+        auto launch = [&](auto k) {
+          set_smem(k, ColTma<LL>::smem());
+          k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
+              tm, dst, ncols, n_ct, n_tiles, box_rows, ncopy, dst_rows,
+              in_add, in_count, out_add, out_count, roots, colrange, err);
+        };
+        if (paired)
+          launch(k_fft_cols_tma<LL, INV, true>);
+        else
+          launch(k_fft_cols_tma<LL, INV, false>);
         GN_LAUNCH_CHECK("pruned column transform (tensor-copy tiles)");
         done = true;
       }
     });
   if (done)
     return;
+  if (paired)
+    throw Error(kInternal, "interleaved coil pairs need the tensor-copy pass");
   with_length(L, [&](auto lc) {
     constexpr int LL = decltype(lc)::value;
     using S = Shape<LL>;
@@ -785,7 +833,7 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
-                           const uint2 *zrange, int *err)
+                           const uint2 *zrange, int *err, bool paired)
 {
   const long long N = g.img_count;
   const long long rows = (long long)g.N[1] * g.N[2];
@@ -827,7 +875,7 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                 g.G[2], C,
                 pos_mod((long long)g.shift_inv[2] - g.crop[2], g.G[2]),
                 g.N[2], pos_mod(-(long long)g.shift_fwd[2], g.G[2]), g.G[2],
-                roots[2], s, zrange, err);
+                roots[2], s, zrange, err, paired);
 }
 
 void launch_pruned_adjoint(const float2 *grid, const float *deapo,

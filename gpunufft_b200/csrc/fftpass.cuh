@@ -47,12 +47,16 @@ size_t pruned_scratch_b(const Geo &g, int C);
 // others are left as they are (the interpolation never reads them).
 // err (optional): the mapped error flag of the tensor-copy passes (set when
 // a tile copy does not complete within its bounded wait); without it the
-// passes load their tiles with plain loads.
+// passes load their tiles with plain loads.  paired (3-D, needs err and
+// every grid axis <= 256): the grid is written with coil pairs interleaved,
+// cell q of coil c at ((c / 2) * G + q) * 2 + c % 2 (C rounded up to even
+// coils of storage).
 void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
-                           const uint2 *zrange = nullptr, int *err = nullptr);
+                           const uint2 *zrange = nullptr, int *err = nullptr,
+                           bool paired = false);
 
 // Adjoint: grid [C][G] (INVERSE fftshift folded in by the adjoint spread)
 // -> unnormalised inverse DFT -> crop of the second INVERSE fftshift ->

@@ -1119,17 +1119,27 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
-// The same interpolation with every coil group of an item in one block (3-D,
-// tiles copied by TMA or, where they wrap, gathered): each thread computes
-// the footprints of its (at most two) samples once, in registers, and the
-// block walks the coil groups through a ring of `nbuf` tile buffers; the
-// copy of group g + nbuf is issued as soon as group g's buffer is released,
-// so nbuf - 1 copies overlap each group's accumulation.  Per sample and coil
-// the arithmetic (cell order z, y, x; weight (wz * wy) * wx; one fused
-// multiply-add per cell) is that of k_forward_tma.
-// Shared memory: nbuf tiles [CG][pad][pad][PX] | nbuf mbarriers | flag.
+// The same interpolation with every coil group of an item in one block (3-D
+// grids written with coil pairs interleaved, cell q of coil c at
+// ((c / 2) * G + q) * 2 + c % 2): each thread computes the footprints of
+// its (at most two) samples once, in registers, and the block walks the
+// coil groups through a ring of `nbuf` tile buffers; the copy of group
+// g + nbuf is issued as soon as group g's buffer is released, so nbuf - 1
+// copies overlap each group's accumulation.  A tile is one 5-D box {2 coils,
+// pad, pad, pad, CG / 2 pairs}: its innermost extent is a coil pair (16
+// bytes), so the sector's x start needs no rounding, and one 16-byte shared
+// load reads two coils of a cell.  Per sample and coil the arithmetic
+// (cell order z, y, x; weight (wz * wy) * wx; one fused multiply-add per
+// cell) is that of k_forward_tma.
+// Shared memory: nbuf tiles [CG / 2][pad][pad][pad][2] | nbuf mbarriers |
+// flag.
 constexpr int kFwdSpt = (kFwdItemSamples + kThreads - 1) / kThreads;
-constexpr int kFwdMaxBufs = 8;
+
+// Tile buffers of the coil-pair kernel start on 128-byte boundaries.
+__host__ __device__ constexpr int pair_tile_stride(int pad)
+{
+  return (2 * pad * pad * pad * 16 + 127) / 128 * 8;  // in float4
+}
 
 template <int CG, int KS, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB)
@@ -1140,16 +1150,20 @@ __global__ void __launch_bounds__(kThreads, MINB)
                          const float *__restrict__ dens,
                          const float2 *__restrict__ grid, Geo g,
                          const float *__restrict__ lut, uint32_t M, int C,
-                         int PX, int nbuf, float scale,
-                         float2 *__restrict__ out, int *__restrict__ err)
+                         int nbuf, float scale, float2 *__restrict__ out,
+                         int *__restrict__ err)
 {
+  static_assert(CG % 2 == 0, "coil pairs");
+  constexpr int NP = CG / 2;  // coil pairs per group
   extern __shared__ __align__(128) unsigned char smraw[];
   const int pad = g.pad;
-  const int cstride = pad * pad * PX;  // elements per coil
-  const int tile_elems = CG * cstride;
-  float2 *tiles = reinterpret_cast<float2 *>(smraw);
+  const int pstride = pad * pad * pad;  // cells per pair
+  const int tile_cells = NP * pstride;
+  static_assert(NP == 2, "buffer stride sized for two pairs");
+  const int tstride = pair_tile_stride(pad);  // >= tile_cells
+  float4 *tiles = reinterpret_cast<float4 *>(smraw);
   uint64_t *mbar = reinterpret_cast<uint64_t *>(
-      smraw + (size_t)nbuf * tile_elems * sizeof(float2));
+      smraw + (size_t)nbuf * tstride * sizeof(float4));
   int &s_fail = *reinterpret_cast<int *>(mbar + nbuf);
   const FwdItem it = items[blockIdx.x];
   const int ng = (C + CG - 1) / CG;
@@ -1158,26 +1172,27 @@ __global__ void __launch_bounds__(kThreads, MINB)
   int base[3];
   for (int a = 0; a < 3; ++a)
     base[a] = sa[a] * g.sw + (g.sw >> 1) - g.offset;
-  const int x0 = base[0] & ~1;  // even start (floor, negative included)
-  const int dx = base[0] - x0;
+  constexpr int dx = 0;  // the box starts at the sector's own x
   bool inside = true;
   for (int a = 0; a < 3; ++a)
     inside = inside && base[a] >= 0 && base[a] + pad <= g.G[a];
   const uint32_t bar_base = smem_addr(mbar);
-  const uint32_t tbytes = (uint32_t)(tile_elems * sizeof(float2));
+  const uint32_t tbytes = (uint32_t)(tile_cells * sizeof(float4));
   const uint64_t tm = reinterpret_cast<uint64_t>(&tmap);
   auto issue = [&](int gi) {  // thread 0: copy coil group gi's tile
     const int b = gi % nbuf;
     const uint32_t bar = bar_base + 8u * (uint32_t)b;
-    const uint32_t dst = smem_addr(tiles + (size_t)b * tile_elems);
+    const uint32_t dst = smem_addr(tiles + (size_t)b * tstride);
     asm volatile(
         "mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
         "r"(tbytes)
         : "memory");
     asm volatile(
-        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::"
-        "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
-        "l"(tm), "r"(x0), "r"(base[1]), "r"(base[2]), "r"(gi * CG), "r"(bar)
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::"
+        "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(
+            dst),
+        "l"(tm), "r"(0), "r"(base[0]), "r"(base[1]), "r"(base[2]),
+        "r"(gi * NP), "r"(bar)
         : "memory");
   };
   if (inside && threadIdx.x == 0)
@@ -1221,7 +1236,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
   for (int gi = 0; gi < ng; ++gi)
   {
     const int buf = inside ? gi % nbuf : 0;
-    const float2 *tile = tiles + (size_t)buf * tile_elems;
+    const float4 *tile = tiles + (size_t)buf * tstride;
     if (inside)
     {
       // the k-th use of a buffer completes phase k of its barrier
@@ -1245,24 +1260,30 @@ __global__ void __launch_bounds__(kThreads, MINB)
       }
     }
     else
-    {  // a tile that wraps around the grid edge: plain loads
-      float2 *dst = tiles;
+    {  // a tile that wraps around the grid edge: plain loads (a pair of
+       // coils per 16 bytes; the second coil of an odd last pair is zero)
+      float4 *dst = tiles;
       const long long G = g.grid_count;
-      for (int e = threadIdx.x; e < tile_elems; e += kThreads)
+      for (int e = threadIdx.x; e < tile_cells; e += kThreads)
       {
-        const int c = e / cstride;
-        int r = e - c * cstride;
-        const int z = r / (pad * PX);
-        r -= z * pad * PX;
-        const int y = r / PX, x = r - y * PX;
-        float2 v = make_float2(0.f, 0.f);
-        if (gi * CG + c < C)
+        const int pr = e / pstride;
+        int r = e - pr * pstride;
+        const int z = r / (pad * pad);
+        r -= z * pad * pad;
+        const int y = r / pad, x = r - y * pad;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        const int c = gi * CG + 2 * pr;
+        if (c < C)
         {
-          int q[3] = {x0 + x, base[1] + y, base[2] + z};
+          int q[3] = {base[0] + x, base[1] + y, base[2] + z};
           for (int a = 0; a < 3; ++a)
             q[a] = ((q[a] % g.G[a]) + g.G[a]) % g.G[a];
-          v = __ldg(grid + (long long)(gi * CG + c) * G +
-                    ((long long)q[2] * g.G[1] + q[1]) * g.G[0] + q[0]);
+          const long long cell =
+              ((long long)q[2] * g.G[1] + q[1]) * g.G[0] + q[0];
+          v = __ldg(reinterpret_cast<const float4 *>(grid) +
+                    (long long)(c >> 1) * G + cell);
+          if (c + 1 >= C)
+            v.z = v.w = 0.f;
         }
         dst[e] = v;
       }
@@ -1295,7 +1316,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
             if (k == y)
               wyv = w[s][1][k];
           const float wzy = __fmul_rn(wzv, wyv);
-          const int row = ((l0[s][2] + z) * pad + l0[s][1] + y) * PX + xb;
+          const int row = ((l0[s][2] + z) * pad + l0[s][1] + y) * pad + xb;
 #pragma unroll
           for (int x = 0; x < KS; ++x)
           {
@@ -1303,11 +1324,13 @@ __global__ void __launch_bounds__(kThreads, MINB)
               break;
             const float wt = __fmul_rn(wzy, w[s][0][x]);
 #pragma unroll
-            for (int c = 0; c < CG; ++c)
+            for (int pr = 0; pr < NP; ++pr)
             {
-              const float2 v = tile[c * cstride + row + x];
-              acc[c].x = __fmaf_rn(v.x, wt, acc[c].x);
-              acc[c].y = __fmaf_rn(v.y, wt, acc[c].y);
+              const float4 v = tile[pr * pstride + row + x];
+              acc[2 * pr].x = __fmaf_rn(v.x, wt, acc[2 * pr].x);
+              acc[2 * pr].y = __fmaf_rn(v.y, wt, acc[2 * pr].y);
+              acc[2 * pr + 1].x = __fmaf_rn(v.z, wt, acc[2 * pr + 1].x);
+              acc[2 * pr + 1].y = __fmaf_rn(v.w, wt, acc[2 * pr + 1].y);
             }
           }
         }
@@ -1736,15 +1759,67 @@ void launch_forward_interp(const FwdItem *items, int n_items,
 using tma::EncodeTiledFn;
 using tma::encode_fn;
 
+bool forward_pairs(const Geo &g, int tile_coils)
+{
+  // 3-D, the z transform with tensor-copy tiles (every axis <= 256), kernel
+  // width <= 3 (four footprint slots), tiles of four coils, two pairs of
+  // tiles within three blocks' shared memory per SM
+  if (g.dim != 3 || slots_for(g) != 4 || !encode_fn())
+    return false;
+  for (int a = 0; a < 3; ++a)
+    if (g.G[a] > 256 || g.G[a] < 16)
+      return false;
+  if (tile_coils > 0 && tile_coils != 4)
+    return false;
+  const size_t tile = (size_t)pair_tile_stride(g.pad) * 16;
+  return 2 * tile + 64 <= 74 * 1024;
+}
+
 bool launch_forward_interp_tma(const FwdItem *items, int n_items,
                                const float *traj_sorted, const uint32_t *idx,
                                const float *dens_sorted, const float2 *grid,
                                const Geo &g, const float *lut, uint32_t M,
                                int C, float scale, float2 *out, int *err,
-                               cudaStream_t s, int tile_coils)
+                               cudaStream_t s, int tile_coils, bool paired)
 {
   if (n_items <= 0)
     return true;
+  if (paired)
+  {  // coil-pair grid: every coil group of an item in one block, a ring of
+     // two tile buffers, three blocks per SM
+    EncodeTiledFn enc = encode_fn();
+    if (!enc)
+      return false;
+    const int pad = g.pad;
+    const int pairs = (C + 1) / 2;
+    CUtensorMap tm;
+    cuuint64_t dims[5] = {2, (cuuint64_t)g.G[0], (cuuint64_t)g.G[1],
+                          (cuuint64_t)g.G[2], (cuuint64_t)pairs};
+    cuuint64_t strides[4];
+    strides[0] = 2 * sizeof(float2);
+    strides[1] = strides[0] * g.G[0];
+    strides[2] = strides[1] * g.G[1];
+    strides[3] = strides[2] * g.G[2];
+    cuuint32_t box[5] = {2, (cuuint32_t)pad, (cuuint32_t)pad,
+                         (cuuint32_t)pad, 2};
+    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, const_cast<float2 *>(grid),
+            dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      throw Error(kInternal, "coil-pair grid tensor map rejected");
+    const int nbuf = 2;
+    const size_t tile = (size_t)pair_tile_stride(pad) * sizeof(float4);
+    const size_t smem2 = (size_t)nbuf * tile + 8 * nbuf + 16;
+    auto k = k_forward_tma_groups<4, 4, 3>;
+    GN_CUDA(cudaFuncSetAttribute(
+        k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
+    k<<<(unsigned)n_items, kThreads, smem2, s>>>(tm, items, traj_sorted, idx,
+                                                dens_sorted, grid, g, lut, M,
+                                                C, nbuf, scale, out, err);
+    GN_LAUNCH_CHECK("forward interpolation (coil-pair tiles, all groups)");
+    return true;
+  }
   EncodeTiledFn enc = encode_fn();
   if (!enc || (g.G[0] & 1))
     return false;
@@ -1794,40 +1869,6 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
     return false;
   const int ks = slots_for(g);
-  if (g.dim == 3 && ks == 4 && 2 * tile + 128 <= 200 * 1024)
-  {  // every coil group of an item in one block: a ring of tile buffers,
-     // as many as fit three blocks per SM (74 KB), at least two
-    int nbuf = (int)((74 * 1024 - 128) / tile);
-    nbuf = std::max(2, std::min(nbuf, kFwdMaxBufs));
-    const int ng = (C + cg - 1) / cg;
-    nbuf = std::min(nbuf, std::max(2, ng));
-    const size_t smem2 = (size_t)nbuf * tile + 8 * nbuf + 16;
-    const bool three = smem2 <= 74 * 1024;
-    auto launch = [&](auto kern) {
-      GN_CUDA(cudaFuncSetAttribute(
-          kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-      kern<<<(unsigned)n_items, kThreads, smem2, s>>>(
-          tm, items, traj_sorted, idx, dens_sorted, grid, g, lut, M, C, PX,
-          nbuf, scale, out, err);
-    };
-    switch (cg)
-    {
-    case 1:
-      if (three) launch(k_forward_tma_groups<1, 4, 3>);
-      else launch(k_forward_tma_groups<1, 4, 2>);
-      break;
-    case 2:
-      if (three) launch(k_forward_tma_groups<2, 4, 3>);
-      else launch(k_forward_tma_groups<2, 4, 2>);
-      break;
-    default:
-      if (three) launch(k_forward_tma_groups<4, 4, 3>);
-      else launch(k_forward_tma_groups<4, 4, 2>);
-      break;
-    }
-    GN_LAUNCH_CHECK("forward interpolation (tensor-copy tiles, all groups)");
-    return true;
-  }
   const dim3 grd((unsigned)n_items, (unsigned)((C + cg - 1) / cg));
 #define GN_TMA(D, CGV, KSV)                                                    \
   {                                                                            \

@@ -101,6 +101,13 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
                                const float *dens_sorted, const float2 *grid,
                                const Geo &g, const float *lut, uint32_t M,
                                int C, float scale, float2 *out, int *err,
-                               cudaStream_t s, int tile_coils = 0);
+                               cudaStream_t s, int tile_coils = 0,
+                               bool paired = false);
+
+// Whether the 3-D forward of this geometry runs on a grid written with coil
+// pairs interleaved (cell q of coil c at ((c / 2) * G + q) * 2 + c % 2;
+// launch_pruned_forward(paired) writes it, launch_forward_interp_tma(paired)
+// reads it).
+bool forward_pairs(const Geo &g, int tile_coils);
 
 }  // namespace gnufft

@@ -684,9 +684,13 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
         throw Error(kNotSupported,
                     "DENSITY_ESTIMATION forward needs grid == image (osf 1)");
   }
-  p.grid.ensure((size_t)C * g.grid_count * sizeof(float2));
-  float2 *grid = p.grid.as<float2>();
   const bool dens_est = stage == GNUFFT_DENSITY_ESTIMATION;
+  // 3-D pruned path: the grid holds coil pairs interleaved
+  const bool paired = p.pruned && !dens_est && p.copy_err_d &&
+                      forward_pairs(g, p.fwd_tile_coils);
+  p.grid.ensure((size_t)(paired ? (C + 1) / 2 * 2 : C) * g.grid_count *
+                sizeof(float2));
+  float2 *grid = p.grid.as<float2>();
   if (p.pruned && !dens_est)
   {  // sens, deapodization, pad, shift and the transform in g.dim passes
     check_copy_err(p);
@@ -697,7 +701,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
     launch_pruned_forward(img, sens, p.deapo.as<float>(), g, (int)C,
                           root_ptrs(p).data(), p.fft_a.as<float2>(),
                           p.fft_b.as<float2>(), grid, s,
-                          p.zrange.as<uint2>(), p.copy_err_d);
+                          p.zrange.as<uint2>(), p.copy_err_d, paired);
     p.launches += g.dim;
     p.mark(5, s);
     p.mark(2, s);
@@ -707,7 +711,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
             p.traj_sorted.as<float>(), p.di.as<uint32_t>(),
             p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
             p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, p.copy_err_d, s,
-            p.fwd_tile_coils))
+            p.fwd_tile_coils, paired))
       launch_forward_interp(
           p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
           p.di.as<uint32_t>(),
