@@ -126,7 +126,19 @@ __device__ __forceinline__ void col_tile_issue(const CUtensorMap *tmap,
 
 // The in-place transform of column cl of tile B; returns the stage-2
 // outputs of thread lt (< R1) in b (outputs k = lt + R1 * k2).
-template <int L, bool INV>
+// Tile position of (row r, column lane cl): rows of TC columns, or (PAIRS)
+// two planes of L rows x TC / 2 columns (lanes cl < TC / 2 in the first).
+template <int L, bool PAIRS>
+__device__ __forceinline__ int col_pos(int r, int cl)
+{
+  constexpr int TC = Shape<L>::TC;
+  if constexpr (PAIRS)
+    return ((cl / (TC / 2)) * L + r) * (TC / 2) + cl % (TC / 2);
+  else
+    return r * TC + cl;
+}
+
+template <int L, bool INV, bool PAIRS = false>
 __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
                                              int in_add, int in_count,
                                              const float2 (&w)[Rm<L>::V / 2],
@@ -134,7 +146,6 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
                                              float2 (&b)[Shape<L>::R2])
 {
   using S = Shape<L>;
-  constexpr int TC = S::TC;
   if (lt < S::R2)
   {
     float2 a[S::R1];
@@ -142,7 +153,7 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
     for (int j = 0; j < S::R1; ++j)
     {
       const int r = (lt + S::R2 * j + in_add) & (L - 1);
-      a[j] = r < in_count ? B[r * TC + cl] : make_float2(0.f, 0.f);
+      a[j] = r < in_count ? B[col_pos<L, PAIRS>(r, cl)] : make_float2(0.f, 0.f);
     }
     reg_fft<S::R1, Rm<L>::V, INV>(a, w);
     const int rho = (lt + in_add) & (S::R2 - 1);
@@ -157,7 +168,7 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
           r.y = -r.y;
         v = cmul(v, r);
       }
-      B[(k1 * S::R2 + rho) * TC + cl] = v;
+      B[col_pos<L, PAIRS>(k1 * S::R2 + rho, cl)] = v;
     }
   }
   __syncthreads();
@@ -165,7 +176,8 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
   {
 #pragma unroll
     for (int u = 0; u < S::R2; ++u)
-      b[u] = B[(lt * S::R2 + ((u + in_add) & (S::R2 - 1))) * TC + cl];
+      b[u] = B[col_pos<L, PAIRS>(lt * S::R2 + ((u + in_add) & (S::R2 - 1)),
+                                  cl)];
     reg_fft<S::R2, Rm<L>::V, INV>(b, w);
   }
 }
@@ -175,35 +187,14 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
 // planes 2p, 2p + 1 of the same columns, so that the two halves of every
 // interleaved output pair are written close in time); an odd last plane
 // follows on its own.
-template <bool PAIRED>
-__device__ __forceinline__ void col_tile_of(long long t, long long n_ct,
-                                            long long planes, long long &plane,
-                                            long long &ct)
-{
-  if (!PAIRED)
-  {
-    plane = t / n_ct;
-    ct = t - plane * n_ct;
-    return;
-  }
-  const long long paired = n_ct * (planes & ~1LL);
-  if (t < paired)
-  {
-    const long long pr = t / (2 * n_ct), rem = t - pr * 2 * n_ct;
-    ct = rem >> 1;
-    plane = 2 * pr + (rem & 1);
-  }
-  else
-  {
-    plane = planes - 1;
-    ct = t - paired;
-  }
-}
-
-// PAIRED: output element (plane c, row r, column col) at
-// ((c / 2) * dst_rows * ncols + r * ncols + col) * 2 + c % 2, i.e. coil
-// pairs interleaved (the layout the 3-D forward interpolation reads two
-// coils of a cell from with one 16-byte load).
+// PAIRED: a tile holds TC / 2 columns of both planes (coils) of a pair,
+// copied as two boxes into two planes of L rows; output element (plane c,
+// row r, column col) goes to ((c / 2) * dst_rows * ncols + r * ncols + col)
+// * 2 + c % 2, i.e. coil pairs interleaved (the layout the 3-D forward
+// interpolation reads two coils of a cell from with one 16-byte load), and
+// every warp store covers TC / 2 whole pairs.  Tile t: pair t / n_ct,
+// column tile t % n_ct (n_ct counted in TC / 2 columns); the second plane of
+// an odd last pair is an out-of-range box (zero fill).
 template <int L, bool INV, bool PAIRED>
 __global__ void __launch_bounds__(Shape<L>::CT, 3)
     k_fft_cols_tma(const __grid_constant__ CUtensorMap tmap,
@@ -225,13 +216,21 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
   const uint32_t buf0 = tma::smem_addr(buf);
   const uint32_t bytes = (uint32_t)(ncopy * box_rows) * 128u;
   const long long stride = gridDim.x;
-  const long long planes = n_tiles / n_ct;
+  constexpr int CW = PAIRED ? TC / 2 : TC;  // columns per tile
   auto issue = [&](long long t, int b) {
-    long long plane, ct;
-    col_tile_of<PAIRED>(t, n_ct, planes, plane, ct);
-    col_tile_issue(&tmap, buf0 + (uint32_t)b * (uint32_t)T::tile_bytes,
-                   bar0 + 8u * (uint32_t)b, (int)ct * TC, (int)plane,
-                   box_rows, ncopy, bytes);
+    const long long pl = t / n_ct, ct = t - pl * n_ct;
+    const uint32_t dst = buf0 + (uint32_t)b * (uint32_t)T::tile_bytes;
+    const uint32_t bar = bar0 + 8u * (uint32_t)b;
+    if (PAIRED)
+    {  // both planes of pair pl, each into its own L rows
+      tma::mbar_expect_tx(bar, bytes);  // two boxes of half the columns
+      tma::copy_3d(dst, &tmap, (int)ct * CW, 0, (int)(2 * pl), bar);
+      tma::copy_3d(dst + (uint32_t)(L * CW * sizeof(float2)), &tmap,
+                   (int)ct * CW, 0, (int)(2 * pl + 1), bar);
+    }
+    else
+      col_tile_issue(&tmap, dst, bar, (int)ct * TC, (int)pl, box_rows, ncopy,
+                     bytes);
   };
   if (threadIdx.x == 0)
   {
@@ -270,16 +269,16 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
       }
       return;
     }
-    long long plane, ct;
-    col_tile_of<PAIRED>(t, n_ct, planes, plane, ct);
-    const long long col = ct * TC + cl;
+    const long long pl = t / n_ct, ct = t - pl * n_ct;
+    const long long plane = PAIRED ? 2 * pl + cl / CW : pl;
+    const long long col = ct * CW + cl % CW;
     uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
     if (colrange && col < ncols)
       cr = __ldg(colrange + col);
     const bool on = col < ncols && cr.x <= cr.y;
     float2 bv[S::R2];
-    col_tile_fft<L, INV>(buf + (size_t)b * L * TC, cl, lt, in_add, in_count,
-                         w, tw, bv);
+    col_tile_fft<L, INV, PAIRED>(buf + (size_t)b * L * TC, cl, lt, in_add,
+                                 in_count, w, tw, bv);
     if (lt < S::R1 && on)
     {
       const long long psz = (long long)dst_rows * ncols;
@@ -710,7 +709,7 @@ template <class K> void set_smem(K kernel, size_t bytes)
 bool col_tensor_map(CUtensorMap &tm, const float2 *base, long long ncols,
                     int rows, long long plane_stride, long long planes, int TC,
                     int box_rows)
-{
+{  // TC: columns per box (a multiple of 2)
   tma::EncodeTiledFn enc = tma::encode_fn();
   if (!enc || (ncols & 1) || (plane_stride & 1) ||
       (reinterpret_cast<uintptr_t>(base) & 15))
@@ -754,13 +753,17 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
         using S = Shape<LL>;
         const int box_rows = src_rows < 256 ? src_rows : 256;
         const int ncopy = (src_rows + box_rows - 1) / box_rows;
+        // paired: boxes of TC / 2 columns of one plane, two per tile
+        const int cw = paired ? S::TC / 2 : S::TC;
+        if (paired && ncopy != 1)
+          return;
         CUtensorMap tm;
         if (!col_tensor_map(tm, src, ncols, src_rows,
-                            (long long)src_rows * ncols, planes, S::TC,
+                            (long long)src_rows * ncols, planes, cw,
                             box_rows))
           return;
-        const long long n_ct = (ncols + S::TC - 1) / S::TC;
-        const long long n_tiles = n_ct * planes;
+        const long long n_ct = (ncols + cw - 1) / cw;
+        const long long n_tiles = n_ct * (paired ? (planes + 1) / 2 : planes);
         auto launch = [&](auto k) {
           set_smem(k, ColTma<LL>::smem());
           k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
