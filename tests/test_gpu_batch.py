@@ -102,3 +102,21 @@ def test_forward_tile_shapes_agree(tile_coils):
                     device="cuda")
     assert rel_l2(p.forward(x).cpu().numpy(),
                   ref.forward(x).cpu().numpy()) < 1e-6
+
+
+@pytest.mark.parametrize("tile_coils", [1, 2, 4])
+def test_forward_tile_shapes_agree_3d(tile_coils):
+    """3-D: tiles of four coils run on the coil-pair grid, other tile widths
+    on the plain grid; the interpolation arithmetic is the same."""
+    import torch
+
+    import gpunufft_b200 as G
+    from tests.helpers import kooshball_3d
+    traj = np.asarray(kooshball_3d(300, 64), np.float32)
+    dims = (32, 32, 32)
+    ref = G.Plan(traj, dims, 3, 8, 2.0)
+    p = G.Plan(traj, dims, 3, 8, 2.0, tile_coils=tile_coils)
+    x = torch.randn((5,) + ref.img_shape, dtype=torch.complex64,
+                    device="cuda")
+    assert rel_l2(p.forward(x).cpu().numpy(),
+                  ref.forward(x).cpu().numpy()) < 1e-6
