@@ -82,6 +82,7 @@ def estimate_bytes(req: Request) -> int:
     scratch = 8 * M * lanes + 2 * 8 * Cn * G          # sorted k-space, grid,
     scratch += 8 * Cn * G                              # cuFFT work area
     vectors = 8 * Cn * M * 2 + 8 * Cn * N + 8 * N * 6  # data, maps, CG
+    vectors += 8 * Cn * M + 8 * N * 4    # the iteration graph's own buffers
     return int(tables + scratch + vectors)
 
 
