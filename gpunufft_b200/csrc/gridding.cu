@@ -538,9 +538,10 @@ __global__ void __launch_bounds__(kThreads, 3)
 // fftshift of the grid folded into the input index) and only the N_x cropped
 // outputs are written: out [C][G_z][G_y][N_x] (rows in the INVERSE-shifted
 // frame the next passes expect).  The grid itself is never written.
-// With 32 coils per group (L <= 256) the row transforms run in place on the
-// accumulator (coil-swizzled rows, acc_pos), which keeps the block near
-// 72 KB at L = 256 (three blocks per SM).  Shared memory: acc | roots [L] |
+// With 16 or 32 coils per group (L <= 256) the row transforms run in place on
+// the accumulator (coil-swizzled rows, acc_pos), which keeps the block near
+// 72 KB at L = 256 and 32 coils (three blocks per SM), near 40 KB with 16
+// coils (four blocks per SM).  Shared memory: acc | roots [L] |
 // spread scratch (partial sums, offsets), followed, for the other coil
 // groups (acc rows padded to CG + 1), by an exchange area for the
 // transform that overlaps the scratch.
@@ -553,7 +554,7 @@ constexpr int xfft_max_coils(int L)
 template <int CG, int L> struct XfftLayout
 {
   using S = fftcore::Shape<L>;
-  static constexpr bool IP = CG == 32 && L <= 256;
+  static constexpr bool IP = CG >= 16 && L <= 256;
   static constexpr int SR2 = IP ? S::R2 : 0;
   static constexpr int ACC = IP ? L * CG : L * (CG + 1);
   static size_t scratch(int NU)
@@ -572,7 +573,8 @@ template <int CG, int L> struct XfftLayout
 };
 
 template <int CG, int V, int L>
-__global__ void __launch_bounds__(kThreads, L <= 256 ? 3 : 1)
+__global__ void __launch_bounds__(kThreads,
+                                  L <= 256 ? (CG == 16 ? 4 : 3) : 1)
     k_adjoint_spmm_xfft(const uint32_t *__restrict__ row_off,
                         const uint2 *__restrict__ nz,
                         const float2 *__restrict__ ks, int CP, Geo g, int C,
@@ -1965,7 +1967,7 @@ bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
     case 2: go(lc, std::integral_constant<int, 2>(), I()); break;
     case 4: go(lc, std::integral_constant<int, 4>(), I()); break;
     case 8: go(lc, std::integral_constant<int, 8>(), I()); break;
-    case 16: go(lc, std::integral_constant<int, 16>(), I()); break;
+    case 16: go(lc, std::integral_constant<int, 16>(), I2()); break;
     default: go(lc, std::integral_constant<int, 32>(), I2()); break;
     }
   };

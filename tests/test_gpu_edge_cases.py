@@ -2,8 +2,9 @@
 (the fused spread, the coil-pair forward and the tensor-copy transform
 passes): no samples (rejected), a single sample, samples piled into one
 sector (forward work items split, dense grid rows), samples exactly on the
--0.5 edge and just below +0.5 (wrap-around), and 32 coils (one coil group
-of the spread, eight tile groups of the forward).  Tolerance as the other
+-0.5 edge and just below +0.5 (wrap-around), and 12, 16 and 32 coils (one
+16- or 32-coil group of the spread, transformed in place on its
+accumulator; several tile groups of the forward).  Tolerance as the other
 parity tests: 1e-5 relative L2 against the FP64-accumulating oracle."""
 import numpy as np
 import pytest
@@ -77,3 +78,11 @@ def test_thirty_two_coils_3d():
     rng = np.random.default_rng(6)
     traj = rng.uniform(-0.5, 0.5, (3, 3000)).astype(np.float32)
     _check(traj, (16, 16, 16), 32, 7)
+
+
+@pytest.mark.parametrize("dims", [(32, 32), (16, 16, 16)])
+@pytest.mark.parametrize("n_coils", [12, 16])
+def test_sixteen_coil_group(dims, n_coils):
+    rng = np.random.default_rng(8)
+    traj = rng.uniform(-0.5, 0.5, (len(dims), 3000)).astype(np.float32)
+    _check(traj, dims, n_coils, 9)
