@@ -257,8 +257,8 @@ constexpr int kSpmmCells = 64;
 // Position of (cell, coil c) in a spread accumulator of CG coils per cell:
 // rows padded to CG + 1 (SR2 == 0), or rows of CG with the coil index
 // XOR-swizzled by the cell (SR2 = R2 of the row transform that runs in place
-// on the accumulator).  The swizzle flips coil bits 1-3 only, so coil pairs
-// stay adjacent (16-byte stores), and it varies with both cell % SR2 and
+// on the accumulator).  The swizzle flips coil bits 1-3 only (those below
+// CG), so coil pairs stay adjacent (16-byte stores), and it varies with both cell % SR2 and
 // cell / SR2, so that the transform's stage-1 accesses (cells r0 + lt) and
 // stage-2 accesses (cells k1 * SR2 + t) each spread over all banks.
 template <int CG, int SR2>
@@ -269,7 +269,7 @@ __device__ __forceinline__ int acc_pos(int cell, int c)
   else
   {
     const int sw = ((cell % SR2) ^ (cell / SR2)) & 7;
-    return cell * CG + (c ^ (sw << 1));
+    return cell * CG + (c ^ ((sw << 1) & (CG - 1)));
   }
 }
 
@@ -538,10 +538,11 @@ __global__ void __launch_bounds__(kThreads, 3)
 // fftshift of the grid folded into the input index) and only the N_x cropped
 // outputs are written: out [C][G_z][G_y][N_x] (rows in the INVERSE-shifted
 // frame the next passes expect).  The grid itself is never written.
-// With 16 or 32 coils per group (L <= 256) the row transforms run in place on
-// the accumulator (coil-swizzled rows, acc_pos), which keeps the block near
+// With 8, 16 or 32 coils per group (L <= 256) the row transforms run in place
+// on the accumulator (coil-swizzled rows, acc_pos), which keeps the block near
 // 72 KB at L = 256 and 32 coils (three blocks per SM), near 40 KB with 16
-// coils (four blocks per SM).  Shared memory: acc | roots [L] |
+// coils (four blocks per SM) and 22 KB with 8 coils (five blocks per SM, the
+// register limit).  Shared memory: acc | roots [L] |
 // spread scratch (partial sums, offsets), followed, for the other coil
 // groups (acc rows padded to CG + 1), by an exchange area for the
 // transform that overlaps the scratch.
@@ -554,7 +555,7 @@ constexpr int xfft_max_coils(int L)
 template <int CG, int L> struct XfftLayout
 {
   using S = fftcore::Shape<L>;
-  static constexpr bool IP = CG >= 16 && L <= 256;
+  static constexpr bool IP = CG >= 8 && L <= 256;
   static constexpr int SR2 = IP ? S::R2 : 0;
   static constexpr int ACC = IP ? L * CG : L * (CG + 1);
   static size_t scratch(int NU)
@@ -574,7 +575,7 @@ template <int CG, int L> struct XfftLayout
 
 template <int CG, int V, int L>
 __global__ void __launch_bounds__(kThreads,
-                                  L <= 256 ? (CG == 16 ? 4 : 3) : 1)
+                                  L <= 256 ? (CG == 8 ? 5 : (CG == 16 ? 4 : 3)) : 1)
     k_adjoint_spmm_xfft(const uint32_t *__restrict__ row_off,
                         const uint2 *__restrict__ nz,
                         const float2 *__restrict__ ks, int CP, Geo g, int C,
@@ -1966,7 +1967,7 @@ bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
     case 1: go(lc, std::integral_constant<int, 1>(), I()); break;
     case 2: go(lc, std::integral_constant<int, 2>(), I()); break;
     case 4: go(lc, std::integral_constant<int, 4>(), I()); break;
-    case 8: go(lc, std::integral_constant<int, 8>(), I()); break;
+    case 8: go(lc, std::integral_constant<int, 8>(), I2()); break;
     case 16: go(lc, std::integral_constant<int, 16>(), I2()); break;
     default: go(lc, std::integral_constant<int, 32>(), I2()); break;
     }
