@@ -542,7 +542,8 @@ __global__ void __launch_bounds__(kThreads, 3)
 // on the accumulator (coil-swizzled rows, acc_pos), which keeps the block near
 // 72 KB at L = 256 and 32 coils (three blocks per SM), near 40 KB with 16
 // coils (four blocks per SM) and 22 KB with 8 coils (five blocks per SM, the
-// register limit).  Shared memory: acc | roots [L] |
+// register limit).  At L = 512 (padded rows, up to 16 coils, about 108 KB)
+// two blocks share an SM.  Shared memory: acc | roots [L] |
 // spread scratch (partial sums, offsets), followed, for the other coil
 // groups (acc rows padded to CG + 1), by an exchange area for the
 // transform that overlaps the scratch.
@@ -575,7 +576,8 @@ template <int CG, int L> struct XfftLayout
 
 template <int CG, int V, int L>
 __global__ void __launch_bounds__(kThreads,
-                                  L <= 256 ? (CG == 8 ? 5 : (CG == 16 ? 4 : 3)) : 1)
+                                  L <= 256 ? (CG == 8 ? 5 : (CG == 16 ? 4 : 3))
+                                           : (L == 512 ? 2 : 1))
     k_adjoint_spmm_xfft(const uint32_t *__restrict__ row_off,
                         const uint2 *__restrict__ nz,
                         const float2 *__restrict__ ks, int CP, Geo g, int C,
