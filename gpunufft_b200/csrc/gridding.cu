@@ -303,16 +303,29 @@ __device__ __forceinline__ void spmm_accumulate(
   // an equal share of the block's contiguous nonzero range per unit
   const uint32_t len = (E - A + NU - 1) / NU;
   const uint32_t u0 = min(E, A + unit * len), u1 = min(E, u0 + len);
-  // first cell whose range contains u0: count the bounds <= u0 with the
-  // CG lanes of this slot (uniform trip count across the warp)
+  // first cell whose range contains u0: the number of bounds
+  // s_off[1..nxc] <= u0 (nondecreasing).  Slots of 16 or 32 lanes count
+  // them with ballots (nxc / LS steps); narrower slots, for which that
+  // loop is long, by a branchless binary search with the same trip count
+  // in every lane
   int cell = 0;
-  const unsigned slot_bits =
-      (LS == 32 ? 0xffffffffu : ((1u << LS) - 1u)) << (slot * LS);
-  for (int base = 0; base < nxc; base += LS)
+  if constexpr (LS >= 16)
   {
-    const int i = base + cl + 1;
-    const bool le = i <= nxc && s_off[i] <= u0;
-    cell += __popc(__ballot_sync(0xffffffffu, le) & slot_bits);
+    const unsigned slot_bits =
+        (LS == 32 ? 0xffffffffu : ((1u << LS) - 1u)) << (slot * LS);
+    for (int base = 0; base < nxc; base += LS)
+    {
+      const int i = base + cl + 1;
+      const bool le = i <= nxc && s_off[i] <= u0;
+      cell += __popc(__ballot_sync(0xffffffffu, le) & slot_bits);
+    }
+  }
+  else
+  {
+    for (int step = nxc > 0 ? 1 << (31 - __clz(nxc)) : 0; step > 0;
+         step >>= 1)
+      if (cell + step <= nxc && s_off[cell + step] <= u0)
+        cell += step;
   }
   if (ZG && A < u0 && u0 < u1)
   {  // empty cells just before this unit's first cell start at u0
@@ -538,8 +551,8 @@ __global__ void __launch_bounds__(kThreads, 3)
 // fftshift of the grid folded into the input index) and only the N_x cropped
 // outputs are written: out [C][G_z][G_y][N_x] (rows in the INVERSE-shifted
 // frame the next passes expect).  The grid itself is never written.
-// With 8, 16 or 32 coils per group (L <= 256) the row transforms run in place
-// on the accumulator (coil-swizzled rows, acc_pos), which keeps the block near
+// With 4 to 32 coils per group (L <= 256) the row transforms run in place on
+// the accumulator (coil-swizzled rows, acc_pos), which keeps the block near
 // 72 KB at L = 256 and 32 coils (three blocks per SM), near 40 KB with 16
 // coils (four blocks per SM) and 22 KB with 8 coils (five blocks per SM, the
 // register limit).  At L = 512 (padded rows, up to 16 coils, about 108 KB)
@@ -553,10 +566,22 @@ constexpr int xfft_max_coils(int L)
   return L <= 256 ? 32 : (L == 512 ? 16 : 8);
 }
 
+// blocks per SM the spread with the x transform is compiled for (register
+// limit 65536 / (256 x blocks)): as many as its shared memory admits where
+// that spills few or no registers
+constexpr int xfft_min_blocks(int CG, int L)
+{
+  if (L > 256)
+    return L == 512 ? 2 : 1;
+  if (CG == 8)
+    return L == 256 ? 5 : 4;
+  return CG == 16 || CG == 4 ? 4 : 3;
+}
+
 template <int CG, int L> struct XfftLayout
 {
   using S = fftcore::Shape<L>;
-  static constexpr bool IP = CG >= 8 && L <= 256;
+  static constexpr bool IP = CG >= 4 && L <= 256;
   static constexpr int SR2 = IP ? S::R2 : 0;
   static constexpr int ACC = IP ? L * CG : L * (CG + 1);
   static size_t scratch(int NU)
@@ -575,9 +600,7 @@ template <int CG, int L> struct XfftLayout
 };
 
 template <int CG, int V, int L>
-__global__ void __launch_bounds__(kThreads,
-                                  L <= 256 ? (CG == 8 ? 5 : (CG == 16 ? 4 : 3))
-                                           : (L == 512 ? 2 : 1))
+__global__ void __launch_bounds__(kThreads, xfft_min_blocks(CG, L))
     k_adjoint_spmm_xfft(const uint32_t *__restrict__ row_off,
                         const uint2 *__restrict__ nz,
                         const float2 *__restrict__ ks, int CP, Geo g, int C,
@@ -1968,7 +1991,7 @@ bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
     {
     case 1: go(lc, std::integral_constant<int, 1>(), I()); break;
     case 2: go(lc, std::integral_constant<int, 2>(), I()); break;
-    case 4: go(lc, std::integral_constant<int, 4>(), I()); break;
+    case 4: go(lc, std::integral_constant<int, 4>(), I2()); break;
     case 8: go(lc, std::integral_constant<int, 8>(), I2()); break;
     case 16: go(lc, std::integral_constant<int, 16>(), I2()); break;
     default: go(lc, std::integral_constant<int, 32>(), I2()); break;
