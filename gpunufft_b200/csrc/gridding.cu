@@ -1480,96 +1480,89 @@ __device__ __forceinline__ float2 prepare_value(const float2 *__restrict__ image
   return v;
 }
 
+// Block (y chunk, z, coil - c0): rows of tpr threads each (tpr from
+// forward_prepare_tpr), no index division.
 template <bool SENS>
 __global__ void __launch_bounds__(kThreads)
     k_forward_prepare(const float2 *__restrict__ image,
                       const float2 *__restrict__ sens,
-                      const float *__restrict__ deapo, Geo g, int C,
-                      int image_grid, float2 *__restrict__ grid)
+                      const float *__restrict__ deapo, Geo g, int c0,
+                      int image_grid, int tpr, float2 *__restrict__ grid)
 {
   const int X = image_grid ? g.N[0] : g.G[0];
   const int Y = image_grid ? g.N[1] : g.G[1];
   const int Z = image_grid ? g.N[2] : g.G[2];
   const long long N = g.img_count;
   const long long plane = (long long)X * Y * Z;
-  const long long rows = (long long)Y * Z * C;
   const int X2 = X >> 1;  // cell pairs per row
   const bool vec = (X & 1) == 0;
-  // threads per row: one 16-byte store each (or one cell for odd rows)
-  const int work = vec ? X2 : X;
-  const int tpr = work >= kThreads ? kThreads : (work > 0 ? work : 1);
-  const int rpb = kThreads / tpr;  // rows per block pass
+  const int rpb = kThreads / tpr;  // rows per block
   const int lr = threadIdx.x / tpr, lt = threadIdx.x - lr * tpr;
-  if (lr >= rpb)
+  const int y = blockIdx.x * rpb + lr;
+  const int z = blockIdx.y;
+  const int c = c0 + blockIdx.z;
+  if (lr >= rpb || y >= Y)
     return;
-  for (long long r = (long long)blockIdx.x * rpb + lr; r < rows;
-       r += (long long)gridDim.x * rpb)
+  float2 *dst = grid + (long long)c * plane + ((long long)z * Y + y) * X;
+  int py = y, pz = z;
+  if (!image_grid)
   {
-    const int y = (int)(r % Y);
-    const long long rz = r / Y;
-    const int z = (int)(rz % Z);
-    const int c = (int)(rz / Z);
-    float2 *dst = grid + (long long)c * plane + ((long long)z * Y + y) * X;
-    int py = y, pz = z;
-    if (!image_grid)
+    // INVERSE fftshift of the padded grid: shifted[q] = padded[q+floor(G/2)]
+    py = wrap_mod(y + g.shift_inv[1], g.G[1]) - g.crop[1];
+    pz = wrap_mod(z + g.shift_inv[2], g.G[2]) - g.crop[2];
+  }
+  const bool row_in = py >= 0 && py < g.N[1] && pz >= 0 && pz < g.N[2];
+  const long long prow = ((long long)pz * g.N[1] + py) * g.N[0];
+  const long long cN = (long long)c * N;
+  if (vec)
+  {
+    // even rows start on even cells: 16-byte aligned pairs
+    float4 *d4 = reinterpret_cast<float4 *>(dst);
+    for (int j = lt; j < X2; j += tpr)
     {
-      // INVERSE fftshift of the padded grid: shifted[q] = padded[q+floor(G/2)]
-      py = wrap_mod(y + g.shift_inv[1], g.G[1]) - g.crop[1];
-      pz = wrap_mod(z + g.shift_inv[2], g.G[2]) - g.crop[2];
-    }
-    const bool row_in = py >= 0 && py < g.N[1] && pz >= 0 && pz < g.N[2];
-    const long long prow = ((long long)pz * g.N[1] + py) * g.N[0];
-    const long long cN = (long long)c * N;
-    if (vec)
-    {
-      // even rows start on even cells: 16-byte aligned pairs
-      float4 *d4 = reinterpret_cast<float4 *>(dst);
-      for (int j = lt; j < X2; j += tpr)
+      float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (row_in)
       {
-        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (row_in)
+        const int xa = 2 * j;
+        const int pa = image_grid ? xa
+                                  : wrap_mod(xa + g.shift_inv[0], g.G[0]) -
+                                        g.crop[0];
+        const int pb = image_grid ? xa + 1
+                                  : wrap_mod(xa + 1 + g.shift_inv[0],
+                                             g.G[0]) -
+                                        g.crop[0];
+        if (pa >= 0 && pa < g.N[0])
         {
-          const int xa = 2 * j;
-          const int pa = image_grid ? xa
-                                    : wrap_mod(xa + g.shift_inv[0], g.G[0]) -
-                                          g.crop[0];
-          const int pb = image_grid ? xa + 1
-                                    : wrap_mod(xa + 1 + g.shift_inv[0],
-                                               g.G[0]) -
-                                          g.crop[0];
-          if (pa >= 0 && pa < g.N[0])
-          {
-            const float2 v = prepare_value<SENS>(image, sens, deapo, prow + pa,
-                                                 cN);
-            o.x = v.x;
-            o.y = v.y;
-          }
-          if (pb >= 0 && pb < g.N[0])
-          {
-            const float2 v = prepare_value<SENS>(image, sens, deapo, prow + pb,
-                                                 cN);
-            o.z = v.x;
-            o.w = v.y;
-          }
+          const float2 v = prepare_value<SENS>(image, sens, deapo, prow + pa,
+                                               cN);
+          o.x = v.x;
+          o.y = v.y;
         }
-        d4[j] = o;
+        if (pb >= 0 && pb < g.N[0])
+        {
+          const float2 v = prepare_value<SENS>(image, sens, deapo, prow + pb,
+                                               cN);
+          o.z = v.x;
+          o.w = v.y;
+        }
       }
+      d4[j] = o;
     }
-    else
+  }
+  else
+  {
+    for (int x = lt; x < X; x += tpr)
     {
-      for (int x = lt; x < X; x += tpr)
+      float2 v = make_float2(0.f, 0.f);
+      if (row_in)
       {
-        float2 v = make_float2(0.f, 0.f);
-        if (row_in)
-        {
-          const int px = image_grid ? x
-                                    : wrap_mod(x + g.shift_inv[0], g.G[0]) -
-                                          g.crop[0];
-          if (px >= 0 && px < g.N[0])
-            v = prepare_value<SENS>(image, sens, deapo, prow + px, cN);
-        }
-        dst[x] = v;
+        const int px = image_grid ? x
+                                  : wrap_mod(x + g.shift_inv[0], g.G[0]) -
+                                        g.crop[0];
+        if (px >= 0 && px < g.N[0])
+          v = prepare_value<SENS>(image, sens, deapo, prow + px, cN);
       }
+      dst[x] = v;
     }
   }
 }
@@ -1698,9 +1691,9 @@ void launch_adjoint_spmm(const uint32_t *row_off, const uint2 *nz,
   {
   case 1: GN_SPMM(1, 1); break;
   case 2: GN_SPMM(2, 1); break;
-  case 4: GN_SPMM(4, 1); break;
-  case 8: GN_SPMM(8, 1); break;
-  case 16: GN_SPMM(16, 1); break;
+  case 4: GN_SPMM(4, 2); break;
+  case 8: GN_SPMM(8, 2); break;
+  case 16: GN_SPMM(16, 2); break;
   default: GN_SPMM(32, 2); break;
   }
 #undef GN_SPMM
@@ -1726,15 +1719,25 @@ void launch_forward_prepare(const float2 *image, const float2 *sens,
                             const float *deapo, const Geo &g, int C,
                             bool image_grid, float2 *grid, cudaStream_t s)
 {
-  const size_t rows = (size_t)C * (image_grid ? (size_t)g.N[1] * g.N[2]
-                                              : (size_t)g.G[1] * g.G[2]);
-  const unsigned nb = (unsigned)std::min<size_t>(rows, 148 * 32);
-  if (sens)
-    k_forward_prepare<true><<<nb, kThreads, 0, s>>>(image, sens, deapo, g, C,
-                                                    image_grid, grid);
-  else
-    k_forward_prepare<false><<<nb, kThreads, 0, s>>>(image, nullptr, deapo, g,
-                                                     C, image_grid, grid);
+  const int X = image_grid ? g.N[0] : g.G[0];
+  const int Y = image_grid ? g.N[1] : g.G[1];
+  const int Z = image_grid ? g.N[2] : g.G[2];
+  // threads per row: 16-byte stores of cell pairs (single cells for odd
+  // rows), at most 64 threads so that short rows still fill the block
+  const int work = (X & 1) == 0 ? X / 2 : X;
+  const int tpr = work >= 64 ? 64 : (work > 0 ? work : 1);
+  const int rpb = kThreads / tpr;
+  for (int c0 = 0; c0 < C; c0 += 65535)
+  {
+    const dim3 grd((unsigned)((Y + rpb - 1) / rpb), (unsigned)Z,
+                   (unsigned)std::min(C - c0, 65535));
+    if (sens)
+      k_forward_prepare<true><<<grd, kThreads, 0, s>>>(
+          image, sens, deapo, g, c0, image_grid, tpr, grid);
+    else
+      k_forward_prepare<false><<<grd, kThreads, 0, s>>>(
+          image, nullptr, deapo, g, c0, image_grid, tpr, grid);
+  }
   GN_LAUNCH_CHECK("forward prepare");
 }
 
