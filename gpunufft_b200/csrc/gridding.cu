@@ -1480,14 +1480,18 @@ __device__ __forceinline__ float2 prepare_value(const float2 *__restrict__ image
   return v;
 }
 
-// Block (y chunk, z, coil - c0): rows of tpr threads each (tpr from
-// forward_prepare_tpr), no index division.
+// Block (y chunk, z, coil - c0): rows of tpr threads each, no index
+// division.  With signs (grids even along every axis) each cell (x, y, z)
+// is multiplied by (-1)^(x+y+z): the transform then yields the spectrum
+// FORWARD-shifted by G/2 = ceil(G/2) on every axis, whose sector tiles are
+// boxes of the grid.
 template <bool SENS>
 __global__ void __launch_bounds__(kThreads)
     k_forward_prepare(const float2 *__restrict__ image,
                       const float2 *__restrict__ sens,
                       const float *__restrict__ deapo, Geo g, int c0,
-                      int image_grid, int tpr, float2 *__restrict__ grid)
+                      int image_grid, int signs, int tpr,
+                      float2 *__restrict__ grid)
 {
   const int X = image_grid ? g.N[0] : g.G[0];
   const int Y = image_grid ? g.N[1] : g.G[1];
@@ -1514,6 +1518,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool row_in = py >= 0 && py < g.N[1] && pz >= 0 && pz < g.N[2];
   const long long prow = ((long long)pz * g.N[1] + py) * g.N[0];
   const long long cN = (long long)c * N;
+  const bool odd_row = ((y + z) & 1) != 0;
   if (vec)
   {
     // even rows start on even cells: 16-byte aligned pairs
@@ -1545,6 +1550,19 @@ __global__ void __launch_bounds__(kThreads)
           o.z = v.x;
           o.w = v.y;
         }
+        if (signs)
+        {  // cells 2j and 2j + 1 of this row: opposite signs
+          if (odd_row)
+          {
+            o.x = -o.x;
+            o.y = -o.y;
+          }
+          else
+          {
+            o.z = -o.z;
+            o.w = -o.w;
+          }
+        }
       }
       d4[j] = o;
     }
@@ -1561,6 +1579,8 @@ __global__ void __launch_bounds__(kThreads)
                                         g.crop[0];
         if (px >= 0 && px < g.N[0])
           v = prepare_value<SENS>(image, sens, deapo, prow + px, cN);
+        if (signs && (((x & 1) != 0) != odd_row))
+          v = make_float2(-v.x, -v.y);
       }
       dst[x] = v;
     }
@@ -1717,7 +1737,8 @@ void launch_adjoint_finish(const float2 *grid, const float *deapo,
 
 void launch_forward_prepare(const float2 *image, const float2 *sens,
                             const float *deapo, const Geo &g, int C,
-                            bool image_grid, float2 *grid, cudaStream_t s)
+                            bool image_grid, float2 *grid, cudaStream_t s,
+                            bool signs)
 {
   const int X = image_grid ? g.N[0] : g.G[0];
   const int Y = image_grid ? g.N[1] : g.G[1];
@@ -1733,10 +1754,11 @@ void launch_forward_prepare(const float2 *image, const float2 *sens,
                    (unsigned)std::min(C - c0, 65535));
     if (sens)
       k_forward_prepare<true><<<grd, kThreads, 0, s>>>(
-          image, sens, deapo, g, c0, image_grid, tpr, grid);
+          image, sens, deapo, g, c0, image_grid, signs ? 1 : 0, tpr, grid);
     else
       k_forward_prepare<false><<<grd, kThreads, 0, s>>>(
-          image, nullptr, deapo, g, c0, image_grid, tpr, grid);
+          image, nullptr, deapo, g, c0, image_grid, signs ? 1 : 0, tpr,
+          grid);
   }
   GN_LAUNCH_CHECK("forward prepare");
 }

@@ -75,10 +75,13 @@ void launch_adjoint_finish(const float2 *grid, const float *deapo,
 
 // Forward prepare: sens multiply, deapodization, zero pad and INVERSE
 // fftshift into grid [C][G].  With `image_grid` the image is written
-// unpadded and unshifted (DENSITY_ESTIMATION, image-sized grid).
+// unpadded and unshifted (DENSITY_ESTIMATION, image-sized grid).  With
+// `signs` (every G even) cell (x, y, z) is multiplied by (-1)^(x+y+z), so
+// that the forward transform yields the FORWARD-shifted spectrum.
 void launch_forward_prepare(const float2 *image, const float2 *sens,
                             const float *deapo, const Geo &g, int C,
-                            bool image_grid, float2 *grid, cudaStream_t s);
+                            bool image_grid, float2 *grid, cudaStream_t s,
+                            bool signs = false);
 
 // Forward interpolation from grid [C][G] (the raw FFT output; with `shift`
 // the upstream's FORWARD fftshift is folded into the tile gather), scaled by

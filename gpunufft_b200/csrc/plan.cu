@@ -73,6 +73,9 @@ struct gnufft_plan
   bool plain = false;
   int fwd_tile_coils = 0;  // 0: automatic
   bool pruned = false;     // separable pruned transforms instead of cuFFT
+  // cuFFT grids even along every axis: the forward folds its shift into the
+  // prepare pass as signs and reads sector tiles by tensor copies
+  bool fwd_signs = false;
   int *copy_err_h = nullptr;  // set by a tile copy that timed out (mapped)
   int *copy_err_d = nullptr;
 
@@ -331,7 +334,10 @@ void init_common(gnufft_plan &p, const gnufft_desc *d)
     throw Error(kNotSupported, err);
   p.pruned = !p.plain && !(d->flags & GNUFFT_FLAG_CUFFT) &&
              pruned_fft_supported(p.g);
-  if (p.pruned)
+  p.fwd_signs = !p.pruned && !p.plain;
+  for (int a = 0; a < p.g.dim; ++a)
+    p.fwd_signs = p.fwd_signs && p.g.G[a] % 2 == 0;
+  if (p.pruned || p.fwd_signs)
   {
     GN_CUDA(cudaHostAlloc(reinterpret_cast<void **>(&p.copy_err_h),
                           sizeof(int), cudaHostAllocMapped));
@@ -724,9 +730,12 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
     p.mark(7, s);
     return;
   }
+  const bool signs = p.fwd_signs && !dens_est;
+  if (signs)
+    check_copy_err(p);
   p.mark(0, s);
   launch_forward_prepare(img, sens, p.deapo.as<float>(), g, (int)C, dens_est,
-                         grid, s);
+                         grid, s, signs);
   p.launches += 1;
   p.mark(1, s);
   p.mark(4, s);
@@ -740,12 +749,20 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
   }
   p.mark(5, s);
   p.mark(2, s);
-  launch_forward_interp(
-      p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
-      p.di.as<uint32_t>(),
-      (p.has_dens && !dens_est) ? p.dens_sorted.as<float>() : nullptr, grid, g,
-      p.lut.as<float>(), p.M, (int)C, !dens_est,
-      dens_est ? 1.0f : g.fft_scale, k, s, p.fwd_tile_coils);
+  // the signed grid holds the FORWARD-shifted spectrum: tiles are boxes
+  if (!signs ||
+      !launch_forward_interp_tma(
+          p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
+          p.di.as<uint32_t>(),
+          p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
+          p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, p.copy_err_d, s,
+          p.fwd_tile_coils, false))
+    launch_forward_interp(
+        p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
+        p.di.as<uint32_t>(),
+        (p.has_dens && !dens_est) ? p.dens_sorted.as<float>() : nullptr, grid,
+        g, p.lut.as<float>(), p.M, (int)C, !dens_est && !signs,
+        dens_est ? 1.0f : g.fft_scale, k, s, p.fwd_tile_coils);
   p.launches += 1;
   p.mark(3, s);
   p.mark(6, s);
