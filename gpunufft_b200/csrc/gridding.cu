@@ -1045,9 +1045,14 @@ __global__ void __launch_bounds__(kThreads)
     }
     __syncthreads();
     if (s_fail)
-    {  // the copy did not complete: report, do not use the tile
+    {  // the copy did not complete: report, do not use the tile, and give
+       // the copy still in flight a bounded wait before the block's shared
+       // memory is released
       if (threadIdx.x == 0)
+      {
         atomicExch(err, 1);
+        mbar_wait_bounded(bar, 0u);
+      }
       return;
     }
   }

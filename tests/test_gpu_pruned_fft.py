@@ -1,8 +1,11 @@
 """The separable pruned transforms (default when every grid axis is a power
 of two in [16, 1024]) against the cuFFT path of the same plan geometry
 (GNUFFT_FLAG_CUFFT), every output stage, with and without maps, 2-D and
-3-D, isotropic and anisotropic.  Both are FP32 transforms of the same data;
-tolerance 1e-5 relative L2 (observed differences are at rounding level)."""
+3-D, isotropic and anisotropic.  On these even grids the cuFFT path's
+forward folds the FORWARD shift into the prepare pass as (-1)^(x+y+z)
+and reads sector tiles by tensor copies, so this also checks that path.
+Both are FP32 transforms of the same data; tolerance 1e-5 relative L2
+(observed differences are at rounding level)."""
 import numpy as np
 import pytest
 
