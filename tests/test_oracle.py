@@ -134,3 +134,26 @@ def test_operator_matches_direct_nudft():
     got = op.adjoint(k[None])[0] * np.sqrt(op.g.grid_count)
     exact = O.nudft_adjoint(traj, k, (32, 32))[0]
     assert rel_l2(got, exact) < 0.05
+
+
+@pytest.mark.parametrize("dims,osf", [((48, 40), 1.5), ((32, 32), 1.25),
+                                      ((12, 12, 12), 2.0),
+                                      ((20, 20, 10), 1.5)])
+def test_forward_shift_as_signs(dims, osf):
+    """The cuFFT-path forward on grids even along every axis multiplies the
+    transform input by (-1)^(x+y+z) instead of shifting the spectrum: on such
+    grids that equals the oracle's FORWARD shift (ceil(G/2)); with an odd
+    axis it does not, and that path keeps the shifted gather."""
+    g = O.make_geometry(dims, osf, 3, 8)
+    rng = np.random.default_rng(3)
+    x = (rng.standard_normal(g.grid_shape)
+         + 1j * rng.standard_normal(g.grid_shape))
+    axes = tuple(range(-g.dim, 0))
+    shifted = O.fftshift(np.fft.fftn(x, axes=axes), g, inverse=False)
+    idx = np.indices(g.grid_shape).sum(0)
+    signed = np.fft.fftn(x * np.where(idx % 2 == 1, -1.0, 1.0), axes=axes)
+    err = rel_l2(signed, shifted)
+    if all(n % 2 == 0 for n in g.grid_shape):
+        assert err < 1e-12
+    else:
+        assert err > 1e-3
