@@ -116,12 +116,19 @@ class ClockSampler:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.device),
                  "--query-gpu=" + self.Q, "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE,
+                 "-lms", "20"], stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
+            return self
+        # the timed region starts once the sampler reports (at most 5 s)
+        t_end = time.monotonic() + 5.0
+        while (not self.lines and self.proc.poll() is None
+               and time.monotonic() < t_end):
+            time.sleep(0.01)
+        self.lines.clear()
         return self
 
     def _read(self):
