@@ -70,6 +70,10 @@ GN_HD float grid_to_k(int gc, int ax, const Geo &g)
 // coordinate u*W - 0.5, weight quantised to 8 fractional bits
 // (cuda_utils.cuh:27-37 with load2DKernel; the 2-D table of the upstream is
 // the outer product of the 1-D table, so its bilinear lookup factorises).
+// The texture unit derives its 8-bit weight from a coordinate it holds with
+// fewer bits than float, so weights next to a rounding boundary may differ
+// by 1/256 from this model: host code (the deapodization) uses the model,
+// device code uses the texture unit itself (texture_weight).
 GN_HD float lerp_table(const float *tab, int W, float u)
 {
   float x = GN_FSUB(GN_FMUL(u, (float)W), 0.5f);
@@ -82,6 +86,20 @@ GN_HD float lerp_table(const float *tab, int W, float u)
   i1 = i1 < 0 ? 0 : (i1 > W - 1 ? W - 1 : i1);
   float t0 = GN_LDG(tab + i0), t1 = GN_LDG(tab + i1);
   return GN_FADD(GN_FMUL(GN_FSUB(1.0f, a), t0), GN_FMUL(a, t1));
+}
+
+// Weight of the TEXTURE operators at normalised coordinate u = d^2 / R^2:
+// on the device the hardware-filtered fetch from the plan's texture object,
+// exactly the lookup the upstream texture kernels make
+// (cuda_utils.cuh:27-37, std_gpuNUFFT_kernels.cu:49-60: linear filtering,
+// normalised coordinates, clamp); the software model on the host.
+GN_HD float texture_weight(const Geo &g, const float *lut, float u)
+{
+#if defined(__CUDA_ARCH__)
+  if (g.lut_tex)
+    return tex1D<float>((cudaTextureObject_t)g.lut_tex, u);
+#endif
+  return lerp_table(lut, g.lut_len, u);
 }
 
 // One axis of the upstream footprint of a sample with coordinate c that
@@ -129,7 +147,7 @@ GN_HD int axis_footprint(float c, int ax, int sector_ax, const Geo &g,
     float wt;
     if (g.texture)
     {
-      wt = lerp_table(lut, g.lut_len, GN_FMUL(d2, g.radius_sq_inv));
+      wt = texture_weight(g, lut, GN_FMUL(d2, g.radius_sq_inv));
     }
     else
     {

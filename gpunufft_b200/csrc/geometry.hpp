@@ -44,6 +44,10 @@ struct Geo
   float aniso[3];        // G_axis / max G
   int lut_len;
   int texture;           // linear-interpolated LUT, no radius cut
+  // TEXTURE operators on the device: the lookup table as a normalised,
+  // clamp-addressed, linearly filtered texture object (0 on the host side
+  // and for the other operator types)
+  unsigned long long lut_tex;
   int crop[3];           // (uint)(N * (osf - 1) / 2) per axis
   int shift_inv[3];      // floor(G/2): INVERSE fftshift offset
   int shift_fwd[3];      // ceil(G/2): FORWARD fftshift offset

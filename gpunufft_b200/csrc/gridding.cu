@@ -213,7 +213,7 @@ __device__ __forceinline__ int compact_axis(float c, int ax, int sec_ax,
     bool valid = i <= imax && i >= 0;
     float wt;
     if (g.texture)
-      wt = lerp_table(lut, g.lut_len, __fmul_rn(d2, g.radius_sq_inv));
+      wt = texture_weight(g, lut, __fmul_rn(d2, g.radius_sq_inv));
     else
     {
       valid = valid && d2 < g.radius_sq;

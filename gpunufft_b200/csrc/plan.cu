@@ -78,6 +78,9 @@ struct gnufft_plan
   bool fwd_signs = false;
   int *copy_err_h = nullptr;  // set by a tile copy that timed out (mapped)
   int *copy_err_d = nullptr;
+  // TEXTURE operators: the lookup table as a filtered texture
+  cudaArray_t lut_array = nullptr;
+  cudaTextureObject_t lut_tex = 0;
 
   // host copies of the exported tables
   std::vector<float> lut_h, traj_sorted_h, dens_sorted_h, deapo_h;
@@ -124,6 +127,10 @@ struct gnufft_plan
       cudaStreamDestroy(stream);
     if (copy_err_h)
       cudaFreeHost(copy_err_h);
+    if (lut_tex)
+      cudaDestroyTextureObject(lut_tex);
+    if (lut_array)
+      cudaFreeArray(lut_array);
     if (prev >= 0)
       cudaSetDevice(prev);
   }
@@ -313,6 +320,33 @@ void build_items(gnufft_plan &p)
   upload(p.fwd_items, fitems.data(), fitems.size(), p.stream);
 }
 
+// The TEXTURE operators read their kernel table through the texture unit:
+// a 1-D array with normalised coordinates, linear filtering and clamp
+// addressing, the sampler state the upstream gives its 2-D table
+// (std_gpuNUFFT_kernels.cu:49-60; that table is the outer product of the 1-D
+// one, so per-axis fetches give the same filtered weights).
+void make_lut_texture(gnufft_plan &p)
+{
+  const cudaChannelFormatDesc fd = cudaCreateChannelDesc<float>();
+  GN_CUDA(cudaMallocArray(&p.lut_array, &fd, (size_t)p.g.lut_len, 0));
+  GN_CUDA(cudaMemcpy2DToArrayAsync(
+      p.lut_array, 0, 0, p.lut_h.data(), p.lut_h.size() * sizeof(float),
+      p.lut_h.size() * sizeof(float), 1, cudaMemcpyHostToDevice, p.stream));
+  cudaResourceDesc rd;
+  std::memset(&rd, 0, sizeof(rd));
+  rd.resType = cudaResourceTypeArray;
+  rd.res.array.array = p.lut_array;
+  cudaTextureDesc td;
+  std::memset(&td, 0, sizeof(td));
+  td.addressMode[0] = cudaAddressModeClamp;
+  td.filterMode = cudaFilterModeLinear;
+  td.readMode = cudaReadModeElementType;
+  td.normalizedCoords = 1;
+  GN_CUDA(cudaCreateTextureObject(&p.lut_tex, &rd, &td, nullptr));
+  GN_CUDA(cudaStreamSynchronize(p.stream));
+  p.g.lut_tex = (unsigned long long)p.lut_tex;
+}
+
 void init_common(gnufft_plan &p, const gnufft_desc *d)
 {
   validate_desc(d);
@@ -353,6 +387,8 @@ void init_common(gnufft_plan &p, const gnufft_desc *d)
   p.lut_h.resize(p.g.lut_len);
   kernel_lut_fill(p.lut_h.data(), p.g.lut_len, (int)d->kernel_width, d->osf);
   upload(p.lut, p.lut_h.data(), p.lut_h.size(), p.stream);
+  if (p.texture)
+    make_lut_texture(p);
   compute_deapo(p.g, p.lut_h.data(), p.deapo_h);
   sector_centers(p.g, p.centers_h);
 }

@@ -11,10 +11,13 @@
 # oracle/ref_compat.h into the upstream .cu files so they compile under
 # CUDA 12 (legacy texture references were removed; see that header).
 #
-# Usage: oracle/build_ref.sh [UPSTREAM_ROOT]   (default: /root/reference)
+# Usage: oracle/build_ref.sh [UPSTREAM_ROOT]
+#   UPSTREAM_ROOT defaults to $GNUFFT_UPSTREAM_ROOT, else to a checkout named
+#   "reference" next to this repository.
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-UP="${1:-/root/reference}/CUDA"
+DEFAULT_UP="${GNUFFT_UPSTREAM_ROOT:-$(cd "$HERE/../.." && pwd)/reference}"
+UP="${1:-$DEFAULT_UP}/CUDA"
 OUT="$HERE/_ref"
 if [ ! -d "$UP/src" ]; then
   echo "upstream sources not found at $UP" >&2

@@ -54,7 +54,7 @@ def lib() -> ctypes.CDLL:
                                         _I, _I]
         L.refg_create.restype = _P
         L.refg_create.argtypes = [_P, _U, _U, _U, _U, _P, _P, _U, _U, _U, _F,
-                                  _I]
+                                  _I, _I]
         L.refg_adjoint.restype = _I
         L.refg_adjoint.argtypes = [_P, _P, _P, _I]
         L.refg_forward.restype = _I
@@ -144,10 +144,14 @@ def cpu_gridding(data_sorted: np.ndarray, crds_sorted_aos: np.ndarray,
 
 
 class RefGpuOperator:
-    """The upstream operator on the GPU (textures off), host-array calls."""
+    """The upstream operator on the GPU, host-array calls.  ``textures``
+    selects the TEXTURE / BALANCED_TEXTURE operators (the factory's
+    useTextures), which read the kernel table through hardware-filtered
+    texture fetches (texture objects standing in for the legacy references,
+    oracle/ref_compat.h)."""
 
     def __init__(self, traj, img_dims, n_coils, kw=3, sw=8, osf=2.0,
-                 dens=None, sens=None, balance=True):
+                 dens=None, sens=None, balance=True, textures=False):
         self.traj = np.ascontiguousarray(traj, np.float32)
         self.dim, self.M = self.traj.shape
         self.img_dims = tuple(int(v) for v in img_dims)
@@ -161,7 +165,7 @@ class RefGpuOperator:
         self.has_sens = sens is not None
         self.h = lib().refg_create(self.traj.ctypes.data, self.M, w, h, d,
                                    _ptr(dens_c), _ptr(sens_c), self.C, kw, sw,
-                                   osf, int(balance))
+                                   osf, int(balance), int(textures))
         if not self.h:
             raise RuntimeError(lib().refh_last_error().decode())
         self.n_img = int(np.prod([v for v in self.img_dims if v]))

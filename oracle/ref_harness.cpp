@@ -13,9 +13,10 @@
  *    GPU-only deapodization step), and the upstream CPU gridding routine
  *    gpuNUFFT_cpu (cpu/gpuNUFFT_cpu.cpp:3-159) that its unit tests use.
  *  - refg_* (GPU): the upstream operator created exactly like the upstream
- *    Python binding does (python/gpuNUFFT_operator_python_factory.cpp:70-120)
- *    but with textures off (the texture operators cannot be built with
- *    CUDA 12), and its host-array adjoint / forward.
+ *    Python binding does (python/gpuNUFFT_operator_python_factory.cpp:70-120),
+ *    with or without textures (the texture operators run through the
+ *    texture-object stand-ins of oracle/ref_compat.h), and its host-array
+ *    adjoint / forward.
  */
 #include <cstdint>
 #include <cstring>
@@ -208,7 +209,7 @@ struct RefOp
 void *refg_create(const float *traj, uint32_t M, uint32_t w, uint32_t h,
                   uint32_t d, const float *dens, const float *sens_c64,
                   uint32_t n_coils, uint32_t kw, uint32_t sw, float osf,
-                  int balance)
+                  int balance, int textures)
 {
   try
   {
@@ -218,7 +219,8 @@ void *refg_create(const float *traj, uint32_t M, uint32_t w, uint32_t h,
     r->w = w;
     r->h = h;
     r->d = d;
-    gpuNUFFT::GpuNUFFTOperatorFactory factory(false, true, balance != 0);
+    gpuNUFFT::GpuNUFFTOperatorFactory factory(textures != 0, true,
+                                              balance != 0);
     gpuNUFFT::Dimensions img = make_dims(w, h, d);
     const int dim = d == 0 ? 2 : 3;
     std::vector<float> traj_copy(traj, traj + (size_t)dim * M);

@@ -58,3 +58,17 @@ def rel_l2(a, b):
     a = np.asarray(a, np.complex128).ravel()
     b = np.asarray(b, np.complex128).ravel()
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def spiral_2d(n_interleaves, n_samples, rng):
+    """Variable-density 2-D spiral (radius ~ u^1.6), ``n_interleaves``
+    rotated arms, ``n_samples`` points in total, coords in [-0.5, 0.5)."""
+    per = max(1, n_samples // n_interleaves)
+    u = np.arange(per) / per
+    turns = rng.uniform(6, 14)
+    r = 0.499 * u ** 1.6
+    arms = []
+    for arm in range(n_interleaves):
+        th = 2 * np.pi * (turns * u + arm / n_interleaves)
+        arms.append(np.stack([r * np.cos(th), r * np.sin(th)]))
+    return np.ascontiguousarray(np.concatenate(arms, 1), np.float32)

@@ -9,7 +9,8 @@ import numpy as np
 import pytest
 
 from oracle import nufft_oracle as O
-from tests.helpers import cplx, gaussian_maps, kooshball_3d, radial_2d, rel_l2
+from tests.helpers import (cplx, gaussian_maps, kooshball_3d, radial_2d,
+                           rel_l2, spiral_2d)
 
 pytestmark = pytest.mark.gpu
 
@@ -31,6 +32,8 @@ CASES = [
     ((16, 16, 16), 2.0, 3, 8, lambda r: kooshball_3d(200, 32)),
     ((20, 20, 10), 1.5, 3, 5, lambda r: r.uniform(-0.5, 0.5, (3, 4000))),
     ((12, 12, 12), 2.0, 4, 3, lambda r: r.uniform(-0.5, 0.5, (3, 1500))),
+    # odd 2-D grid (219^2), kw 5, a variable-density spiral
+    ((160, 160), 1.37, 5, 8, lambda r: spiral_2d(24, 40000, r)),
 ]
 
 
@@ -77,7 +80,7 @@ def test_adjoint_forward_vs_oracle(case, n_coils):
     assert rel_l2(got, exp) < TOL, rel_l2(got, exp)
 
 
-@pytest.mark.parametrize("case", [0, 3, 4])
+@pytest.mark.parametrize("case", [0, 3, 4, 6])
 def test_sensitivity_combine(case):
     dims, osf, kw, sw, mk = CASES[case]
     rng = np.random.default_rng(200 + case)
@@ -93,6 +96,17 @@ def test_sensitivity_combine(case):
     assert rel_l2(p.forward(x), ref.forward(x[None])) < TOL
 
 
+# The TEXTURE operators weight with the texture unit's filtered fetch, as
+# the upstream does; the oracle restates that filtering as 8-bit weights
+# computed from the float texel coordinate.  The unit derives its weight
+# from a coordinate held with fewer bits, so weights next to a rounding
+# boundary differ by 1/256 from the model: 1-3e-5 relative L2 on these
+# cases, hence 6e-5 here.  The strict pin of these operators (1e-5) is the
+# upstream's own texture operators run on the texture unit
+# (test_gpu_reference.py).
+TEX_TOL = 6e-5
+
+
 # cases 1 and 5: grids even along every axis but not powers of two (72 x 60,
 # 24^3), whose forward reads sector tiles by tensor copies of the signed
 # cuFFT spectrum
@@ -105,9 +119,9 @@ def test_texture_variants_vs_oracle(case):
     p = _plan(traj, dims, kw, sw, osf, texture=True)
     ref = O.OracleOperator(traj, dims, kw, sw, osf, texture=True)
     k = cplx(rng, 2, M)
-    assert rel_l2(p.adjoint(k), ref.adjoint(k)) < TOL
+    assert rel_l2(p.adjoint(k), ref.adjoint(k)) < TEX_TOL
     x = cplx(rng, 2, *ref.g.img_shape)
-    assert rel_l2(p.forward(x), ref.forward(x)) < TOL
+    assert rel_l2(p.forward(x), ref.forward(x)) < TEX_TOL
 
 
 def test_adjointness_device_tensors():

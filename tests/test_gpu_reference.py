@@ -1,12 +1,13 @@
 """Parity against the upstream library's own GPU run on the same inputs.
 
-The upstream DEFAULT and BALANCED operators are compiled from the upstream
-sources for sm_100a (``oracle/build_ref.sh`` -> ``oracle/_ref``; texture
-operators cannot be built with CUDA 12) and driven through their host-array
-API (``performGpuNUFFTAdj`` / ``performForwardGpuNUFFT``,
+The upstream operators are compiled from the upstream sources for sm_100a
+(``oracle/build_ref.sh`` -> ``oracle/_ref``; the TEXTURE and
+BALANCED_TEXTURE operators run on the texture unit through the
+texture-object stand-ins of ``oracle/ref_compat.h``) and driven through
+their host-array API (``performGpuNUFFTAdj`` / ``performForwardGpuNUFFT``,
 ``gpuNUFFT_operator.hpp:243-345``).  Results of this library must agree
 within 1e-5 relative L2 (both accumulate in FP32; the summation order
-differs).
+differs) for all four operator types.
 
 Only isotropic 2-D geometries are run through the upstream GPU code: its
 2-D forward tests y wrap-around against the grid width
@@ -17,7 +18,8 @@ import numpy as np
 import pytest
 
 from oracle import ref as R
-from tests.helpers import cplx, gaussian_maps, kooshball_3d, radial_2d, rel_l2
+from tests.helpers import (cplx, gaussian_maps, kooshball_3d, radial_2d,
+                           rel_l2, spiral_2d)
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not R.available(),
@@ -47,6 +49,25 @@ CASES = {
     "3d_aniso_uniform_kw4": ((24, 24, 12),
                              lambda r: r.uniform(-0.5, 0.5, (3, 5000)), 2,
                              1.5, 4, 5, "uniform", False),
+    # the differentiable-operator workload: 2-D 256^2, 16 coils, radial
+    # 402 spokes x 512 samples
+    "2d256_radial402x512_16coil_sens": ((256, 256),
+                                        lambda r: radial_2d(402, 512), 16,
+                                        2.0, 3, 8, None, True),
+    # instances of the uneven spiral batch: 160^2, kw 5, 24 interleaves,
+    # 40k samples; osf 1.375 (grid 220^2) with 8 coils, and osf 1.37 (grid
+    # 219^2, odd) with one coil.  The upstream's 2-D shift on a grid with an
+    # odd axis copies ONE coil's grid and then reads every coil of the
+    # chunk from that copy (std_gpuNUFFT_kernels.cu:600-625 with :420-439),
+    # past its end when a chunk holds several coils: odd 2-D grids are run
+    # against the upstream with one coil only (several coils: against the
+    # oracle, test_gpu_operator.py).
+    "2d160_spiral_osf1.375_kw5_8coil": ((160, 160),
+                                        lambda r: spiral_2d(24, 40000, r), 8,
+                                        1.375, 5, 8, "ramp", True),
+    "2d160_spiral_osf1.37_kw5_1coil": ((160, 160),
+                                       lambda r: spiral_2d(24, 40000, r), 1,
+                                       1.37, 5, 8, "ramp", True),
 }
 
 
@@ -64,16 +85,19 @@ def _inputs(name, seed):
     return traj, dims, C, osf, kw, sw, w, maps, rng
 
 
+@pytest.mark.parametrize("textures", [False, True])
 @pytest.mark.parametrize("balanced", [False, True])
 @pytest.mark.parametrize("name", list(CASES))
-def test_matches_upstream_gpu_run(name, balanced):
+def test_matches_upstream_gpu_run(name, balanced, textures):
     import gpunufft_b200 as G
     traj, dims, C, osf, kw, sw, w, maps, rng = _inputs(name, 11)
     M = traj.shape[1]
-    op_type = G.BALANCED if balanced else G.DEFAULT
+    op_type = {(False, False): G.DEFAULT, (False, True): G.BALANCED,
+               (True, False): G.TEXTURE,
+               (True, True): G.BALANCED_TEXTURE}[(textures, balanced)]
     ours = G.Plan(traj, dims, kw, sw, osf, w, maps, op_type)
     up = R.RefGpuOperator(traj, dims, C, kw, sw, osf, dens=w, sens=maps,
-                          balance=balanced)
+                          balance=balanced, textures=textures)
     up1 = None
     try:
         k = cplx(rng, C, M)
@@ -86,7 +110,7 @@ def test_matches_upstream_gpu_run(name, balanced):
             # output only for the first coil chunk (gpuNUFFT_operator.cpp:
             # 737-740, 800-806): compare those stages on one coil.
             up1 = R.RefGpuOperator(traj, dims, 1, kw, sw, osf, dens=w,
-                                   balance=balanced)
+                                   balance=balanced, textures=textures)
             for stage in (G.CONVOLUTION, G.FFT):
                 got = np.asarray(ours.adjoint(k[:1], stage)).ravel()
                 exp = up1.adjoint(k[:1], stage, out_len=got.size)
@@ -104,7 +128,7 @@ def test_matches_upstream_gpu_run(name, balanced):
             # maps applied to the image, a one-coil upstream operator.
             if up1 is None:
                 up1 = R.RefGpuOperator(traj, dims, 1, kw, sw, osf, dens=w,
-                                       balance=False)
+                                       balance=False, textures=textures)
             xs = [maps[c] * x if maps is not None else x[c]
                   for c in range(C)]
             exp = np.concatenate([up1.forward(v) for v in xs])
@@ -144,3 +168,48 @@ def test_matches_upstream_gpu_run_3d128_32coil():
     finally:
         up.close()
         ours.close()
+
+
+@pytest.mark.parametrize("textures", [False, True])
+@pytest.mark.parametrize("balanced", [False, True])
+@pytest.mark.parametrize("dim", [2, 3])
+def test_density_estimation_matches_upstream(dim, balanced, textures):
+    """DENSITY_ESTIMATION (gpuNUFFT_operator.cpp:735-751 adjoint: the raw
+    grid; :1178-1187 forward: interpolation straight from the deapodized
+    image array, meaningful at osf 1) against the upstream at osf 1, through
+    the NUFFTOp ``adj_op(grid_data=True)`` / ``op(interpolate_data=True)``
+    calls.  The upstream forward returns after its first coil chunk (one
+    coil in 3-D), so only that chunk is compared with it; every coil is
+    compared with the oracle."""
+    import gpunufft_b200 as G
+    from oracle import nufft_oracle as O
+    rng = np.random.default_rng(40 + dim)
+    if dim == 2:
+        dims, traj = (32, 32), radial_2d(24, 64)
+    else:
+        dims, traj = (16, 16, 16), kooshball_3d(100, 32)
+    C = 2
+    M = traj.shape[1]
+    op = G.NUFFTOp(traj, dims, C, None, None, 3, 8, 1,
+                   balance_workload=balanced, use_textures=textures)
+    up = R.RefGpuOperator(traj, dims, C, 3, 8, 1.0, balance=balanced,
+                          textures=textures)
+    ora = O.OracleOperator(traj, dims, 3, 8, 1.0, texture=textures)
+    try:
+        k = cplx(rng, C, M)
+        x = cplx(rng, C, *dims[::-1])
+        N = int(np.prod(dims))
+        got = np.asarray(op.adj_op(k, grid_data=True)).ravel()
+        exp = up.adjoint(k, G.DENSITY_ESTIMATION, out_len=C * N)
+        assert rel_l2(got, exp) < TOL, rel_l2(got, exp)
+        ora_tol = 6e-5 if textures else TOL
+        assert rel_l2(got, ora.adjoint(k, G.DENSITY_ESTIMATION).ravel()) \
+            < ora_tol
+        got = np.asarray(op.op(x.reshape(C, -1), interpolate_data=True))
+        exp = up.forward(x, G.DENSITY_ESTIMATION)
+        first = C if dim == 2 else 1
+        assert rel_l2(got[:first], exp[:first]) < TOL
+        assert rel_l2(got, ora.forward(x, G.DENSITY_ESTIMATION)) < ora_tol
+    finally:
+        up.close()
+        op.plan.close()
