@@ -25,6 +25,8 @@ CONVOLUTION, FFT, DEAPODIZATION, DENSITY_ESTIMATION = 0, 1, 2, 3
 FLAG_REFERENCE_ORDER = 0x1
 FLAG_PLAIN = 0x2
 FLAG_CUFFT = 0x4
+# GNUFFT_NOALLOC_SCRATCH_BYTES: staging area of the no-allocation adjoint
+NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 def fwd_tile_flag(coils: int) -> int:
@@ -44,6 +46,7 @@ EXPORTED = (
     "gnufft_last_error", "gnufft_status_string", "gnufft_version",
     "gnufft_adjoint_convolution_noalloc",
     "gnufft_traj_grad_device", "gnufft_set_sens_device",
+    "gnufft_set_copy_wait", "gnufft_plan_check",
 )
 
 
@@ -135,6 +138,10 @@ def lib() -> ctypes.CDLL:
     L.gnufft_traj_grad_device.restype = st
     L.gnufft_traj_grad_device.argtypes = [_P, _P, _P, _U, _P, _P]
     L.gnufft_set_timing.restype = st
+    L.gnufft_set_copy_wait.restype = ctypes.c_int
+    L.gnufft_set_copy_wait.argtypes = [_P, ctypes.c_int64]
+    L.gnufft_plan_check.restype = ctypes.c_int
+    L.gnufft_plan_check.argtypes = [_P]
     L.gnufft_set_timing.argtypes = [_P, ctypes.c_int]
     L.gnufft_get_stage_times.restype = st
     L.gnufft_get_stage_times.argtypes = [_P, ctypes.POINTER(StageTimes)]

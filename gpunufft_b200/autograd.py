@@ -100,18 +100,34 @@ class NUFFT(torch.nn.Module):
         self.dens = None if dens is None else np.ascontiguousarray(
             torch.as_tensor(dens).detach().cpu().numpy(), np.float32)
         self._plan: Optional[Plan] = None
-        self._traj: Optional[np.ndarray] = None
+        self._traj: Optional[torch.Tensor] = None  # copy the plan was built on
+        self._key = None
 
     def plan_for(self, traj: torch.Tensor) -> Plan:
-        t = np.ascontiguousarray(traj.detach().cpu().numpy(), np.float32)
-        if self._plan is None or not np.array_equal(t, self._traj):
+        """The plan of this trajectory, rebuilt only when it changed.  The
+        same tensor unmodified since the last call (storage, version counter,
+        shape, device) reuses the plan without looking at the values; any
+        other tensor is compared with the plan's trajectory where it lives
+        (on the GPU for CUDA tensors), and only a different trajectory is
+        copied to the host to build a new plan."""
+        t = traj.detach()
+        key = (t.data_ptr(), t._version, tuple(t.shape), t.device)
+        if self._plan is not None and key == self._key:
+            return self._plan
+        same = (self._plan is not None and self._traj is not None and
+                self._traj.shape == t.shape and
+                self._traj.device == t.device and
+                bool(torch.equal(self._traj, t.to(self._traj.dtype))))
+        if not same:
             if self._plan is not None:
                 self._plan.close()
             dev = traj.device.index if traj.is_cuda else 0
-            self._plan = Plan(t, self.img_dims, self.kernel_width,
+            host = np.ascontiguousarray(t.cpu().numpy(), np.float32)
+            self._plan = Plan(host, self.img_dims, self.kernel_width,
                               self.sector_width, self.osf, self.dens,
                               self.sens, self.operator_type, device=dev or 0)
-            self._traj = t
+            self._traj = t.to(torch.float32).clone()
+        self._key = key
         return self._plan
 
     def forward(self, x: torch.Tensor, traj: torch.Tensor) -> torch.Tensor:

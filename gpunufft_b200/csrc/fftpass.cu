@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
                    long long n_tiles, int box_rows, int ncopy, int dst_rows,
                    int in_add, int in_count, int out_add, int out_count,
                    const float2 *__restrict__ roots,
-                   const uint2 *__restrict__ colrange, int *__restrict__ err)
+                   const uint2 *__restrict__ colrange, tma::CopyWait cw)
 {
   using S = Shape<L>;
   using T = ColTma<L>;
@@ -253,7 +253,8 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
   {
     const int b = i & 1;
     if (threadIdx.x == 0 &&
-        !tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b, (uint32_t)(i >> 1) & 1u))
+        !tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b,
+                                (uint32_t)(i >> 1) & 1u, cw.polls))
       s_fail = 1;
     __syncthreads();
     if (s_fail)
@@ -261,7 +262,7 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
        // (this tile's, the next one's) a bounded wait before returning
       if (threadIdx.x == 0)
       {
-        atomicExch(err, 1);
+        atomicExch(cw.err, 1);
         tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b, (uint32_t)(i >> 1) & 1u);
         if (t + stride < n_tiles)
           tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)(b ^ 1),
@@ -741,11 +742,11 @@ template <bool INV>
 void cols(int L, const float2 *src, float2 *dst, long long ncols,
           int src_rows, int dst_rows, long long planes, int in_add,
           int in_count, int out_add, int out_count, const float2 *roots,
-          cudaStream_t s, const uint2 *colrange = nullptr, int *err = nullptr,
-          bool paired = false)
+          cudaStream_t s, const uint2 *colrange = nullptr,
+          tma::CopyWait wait = tma::CopyWait(), bool paired = false)
 {
   bool done = false;
-  if (err && L <= 256)
+  if (wait.err && L <= 256)
     with_length(L, [&](auto lc) {
       constexpr int LL = decltype(lc)::value;
       if constexpr (LL <= 256)
@@ -768,7 +769,7 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
           set_smem(k, ColTma<LL>::smem());
           k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
               tm, dst, ncols, n_ct, n_tiles, box_rows, ncopy, dst_rows,
-              in_add, in_count, out_add, out_count, roots, colrange, err);
+              in_add, in_count, out_add, out_count, roots, colrange, wait);
         };
         if (paired)
           launch(k_fft_cols_tma<LL, INV, true>);
@@ -836,7 +837,8 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
-                           const uint2 *zrange, int *err, bool paired)
+                           const uint2 *zrange, tma::CopyWait cw,
+                           bool paired)
 {
   const long long N = g.img_count;
   const long long rows = (long long)g.N[1] * g.N[2];
@@ -872,13 +874,13 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
               (long long)C * g.N[2],
               pos_mod((long long)g.shift_inv[1] - g.crop[1], g.G[1]), g.N[1],
               pos_mod(-(long long)g.shift_fwd[1], g.G[1]), g.G[1], roots[1],
-              s, nullptr, err);
+              s, nullptr, cw);
   if (g.dim == 3)  // z: B -> grid
     cols<false>(g.G[2], tmp_b, grid, (long long)g.G[1] * g.G[0], g.N[2],
                 g.G[2], C,
                 pos_mod((long long)g.shift_inv[2] - g.crop[2], g.G[2]),
                 g.N[2], pos_mod(-(long long)g.shift_fwd[2], g.G[2]), g.G[2],
-                roots[2], s, zrange, err, paired);
+                roots[2], s, zrange, cw, paired);
 }
 
 void launch_pruned_adjoint(const float2 *grid, const float *deapo,
@@ -941,7 +943,7 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
                                   int stage, int accumulate,
                                   const float2 *const roots[3],
                                   float2 *tmp_b, float2 *part, float2 *out,
-                                  cudaStream_t s, int *err)
+                                  cudaStream_t s, tma::CopyWait cw)
 {
   const long long N = g.img_count;
   const float2 *src = xrows;
@@ -952,7 +954,7 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
     cols<true>(g.G[1], xrows, tmp_b, g.N[0], g.G[1], g.N[1],
                (long long)C * g.G[2], 0, g.G[1],
                pos_mod(-(long long)g.crop[1] - g.shift_inv[1], g.G[1]),
-               g.N[1], roots[1], s, nullptr, err);
+               g.N[1], roots[1], s, nullptr, cw);
     src = tmp_b;
     ncols = (long long)g.N[1] * g.N[0];
     ax = 2;

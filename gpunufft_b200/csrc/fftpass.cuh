@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include "geometry.hpp"
+#include "tma.cuh"
 
 namespace gnufft
 {
@@ -55,7 +56,8 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
-                           const uint2 *zrange = nullptr, int *err = nullptr,
+                           const uint2 *zrange = nullptr,
+                           tma::CopyWait cw = tma::CopyWait(),
                            bool paired = false);
 
 // Adjoint: grid [C][G] (INVERSE fftshift folded in by the adjoint spread)
@@ -79,7 +81,8 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
                                   int stage, int accumulate,
                                   const float2 *const roots[3],
                                   float2 *tmp_b, float2 *part, float2 *out,
-                                  cudaStream_t s, int *err = nullptr);
+                                  cudaStream_t s,
+                                  tma::CopyWait cw = tma::CopyWait());
 size_t pruned_scratch_xfirst(const Geo &g, int C);
 
 }  // namespace gnufft

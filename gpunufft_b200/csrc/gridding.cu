@@ -977,8 +977,7 @@ __global__ void __launch_bounds__(kThreads)
                   const float *__restrict__ dens,
                   const float2 *__restrict__ grid, Geo g,
                   const float *__restrict__ lut, uint32_t M, int C, int PX,
-                  float scale, float2 *__restrict__ out,
-                  int *__restrict__ err)
+                  float scale, float2 *__restrict__ out, tma::CopyWait cw)
 {
   extern __shared__ __align__(128) unsigned char smraw[];
   const int pad = g.pad;
@@ -1032,15 +1031,7 @@ __global__ void __launch_bounds__(kThreads)
     if (threadIdx.x == 0)
     {  // one thread waits (bounded); the others wait at the barrier below,
        // which orders the copied tile before their reads
-      uint32_t done = 0;
-      for (long long i = 0; i < kMbarSpin && !done; ++i)
-        asm volatile(
-            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
-            "[%1], 0; selp.u32 %0, 1, 0, p; }"
-            : "=r"(done)
-            : "r"(bar)
-            : "memory");
-      if (!done)
+      if (!mbar_wait_bounded(bar, 0u, cw.polls))
         s_fail = 1;
     }
     __syncthreads();
@@ -1050,7 +1041,7 @@ __global__ void __launch_bounds__(kThreads)
        // memory is released
       if (threadIdx.x == 0)
       {
-        atomicExch(err, 1);
+        atomicExch(cw.err, 1);
         mbar_wait_bounded(bar, 0u);
       }
       return;
@@ -1184,7 +1175,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
                          const float2 *__restrict__ grid, Geo g,
                          const float *__restrict__ lut, uint32_t M, int C,
                          int nbuf, float scale, float2 *__restrict__ out,
-                         int *__restrict__ err)
+                         tma::CopyWait cw)
 {
   static_assert(CG % 2 == 0, "coil pairs");
   constexpr int NP = CG / 2;  // coil pairs per group
@@ -1275,7 +1266,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
       // the k-th use of a buffer completes phase k of its barrier
       if (threadIdx.x == 0 &&
           !mbar_wait_bounded(bar_base + 8u * (uint32_t)buf,
-                             (uint32_t)(gi / nbuf) & 1u))
+                             (uint32_t)(gi / nbuf) & 1u, cw.polls))
         s_fail = 1;
       __syncthreads();
       if (s_fail)
@@ -1284,7 +1275,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
          // block's shared memory is released
         if (threadIdx.x == 0)
         {
-          atomicExch(err, 1);
+          atomicExch(cw.err, 1);
           for (int q = gi; q < ng && q < gi + nbuf; ++q)
             mbar_wait_bounded(bar_base + 8u * (uint32_t)(q % nbuf),
                               (uint32_t)(q / nbuf) & 1u);
@@ -1837,8 +1828,9 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
                                const float *traj_sorted, const uint32_t *idx,
                                const float *dens_sorted, const float2 *grid,
                                const Geo &g, const float *lut, uint32_t M,
-                               int C, float scale, float2 *out, int *err,
-                               cudaStream_t s, int tile_coils, bool paired)
+                               int C, float scale, float2 *out,
+                               tma::CopyWait cw, cudaStream_t s,
+                               int tile_coils, bool paired)
 {
   if (n_items <= 0)
     return true;
@@ -1874,7 +1866,7 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
         k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
     k<<<(unsigned)n_items, kThreads, smem2, s>>>(tm, items, traj_sorted, idx,
                                                 dens_sorted, grid, g, lut, M,
-                                                C, nbuf, scale, out, err);
+                                                C, nbuf, scale, out, cw);
     GN_LAUNCH_CHECK("forward interpolation (coil-pair tiles, all groups)");
     return true;
   }
@@ -1935,7 +1927,7 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
       GN_CUDA(cudaFuncSetAttribute(                                            \
           k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));         \
     k<<<grd, kThreads, smem, s>>>(tm, items, traj_sorted, idx, dens_sorted,    \
-                                  grid, g, lut, M, C, PX, scale, out, err);    \
+                                  grid, g, lut, M, C, PX, scale, out, cw);     \
   }
 #define GN_TMA_KS(D, CGV)                                                      \
   if (ks == 4)                                                                 \

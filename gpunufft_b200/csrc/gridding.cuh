@@ -7,6 +7,7 @@
 #include <cuda_runtime.h>
 
 #include "geometry.hpp"
+#include "tma.cuh"
 
 namespace gnufft
 {
@@ -95,17 +96,18 @@ void launch_forward_interp(const FwdItem *items, int n_items,
 
 // Forward interpolation with each sector tile fetched by one bulk tensor
 // copy (tiles that wrap around the grid edge by plain loads).  The grid
-// must hold the FORWARD-shifted spectrum (cell q at q).  `err` (device
-// pointer) is set to 1 if a copy did not complete within the bounded wait.
+// must hold the FORWARD-shifted spectrum (cell q at q).  cw.err (device
+// pointer) is set to 1 if a copy did not complete within its bounded wait
+// (cw.polls polls).
 // Returns false when the geometry does not suit tensor copies (nothing is
 // launched then).
 bool launch_forward_interp_tma(const FwdItem *items, int n_items,
                                const float *traj_sorted, const uint32_t *idx,
                                const float *dens_sorted, const float2 *grid,
                                const Geo &g, const float *lut, uint32_t M,
-                               int C, float scale, float2 *out, int *err,
-                               cudaStream_t s, int tile_coils = 0,
-                               bool paired = false);
+                               int C, float scale, float2 *out,
+                               tma::CopyWait cw, cudaStream_t s,
+                               int tile_coils = 0, bool paired = false);
 
 // Whether the 3-D forward of this geometry runs on a grid written with coil
 // pairs interleaved (cell q of coil c at ((c / 2) * G + q) * 2 + c % 2;

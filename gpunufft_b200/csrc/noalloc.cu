@@ -12,7 +12,7 @@
 // (samples x coil lanes), which lives in the fixed array below.  Every GPU
 // that loads this library holds it until the process exits.
 #include <cstdint>
-#include <mutex>
+#include <exception>
 #include <string>
 
 #include <cuda_runtime.h>
@@ -30,30 +30,21 @@ constexpr size_t kScratchElems = kScratchBytes / sizeof(float2);
 // Shared by every call on a device; keeps the contents of the last call.
 static __device__ __align__(256) float2 g_noalloc_ks[kScratchElems];
 
-// Device address of g_noalloc_ks per device ordinal.  In host code the
-// array's name is only a host-side stand-in; the address must come from
-// cudaGetSymbolAddress with the device current.
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-float2 *g_addr[kMaxDevices] = {};
-
-float2 *scratch_address(int device)
+// Device address of g_noalloc_ks on the current device.  In host code the
+// array's name is only a host-side stand-in; the address comes from
+// cudaGetSymbolAddress with the device current, looked up on every call
+// (cheap once the module is loaded; a cached address would go stale after
+// the context is torn down and recreated).
+float2 *scratch_address()
 {
-  if (device < 0 || device >= kMaxDevices)
-    throw gnufft::Error(gnufft::kInvalidArgument, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[device])
-  {
-    void *ptr = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_ks);
-    if (e != cudaSuccess || !ptr)
-      throw gnufft::Error(gnufft::kCudaError,
-                          std::string("cudaGetSymbolAddress(no-allocation "
-                                      "scratch): ") +
-                              cudaGetErrorString(e));
-    g_addr[device] = static_cast<float2 *>(ptr);
-  }
-  return g_addr[device];
+  void *ptr = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_ks);
+  if (e != cudaSuccess || !ptr)
+    throw gnufft::Error(gnufft::kCudaError,
+                        std::string("cudaGetSymbolAddress(no-allocation "
+                                    "scratch): ") +
+                            cudaGetErrorString(e));
+  return static_cast<float2 *>(ptr);
 }
 }  // namespace
 
@@ -64,35 +55,30 @@ extern "C" gnufft_status gnufft_adjoint_convolution_noalloc(gnufft_plan *plan,
                                                             void *stream)
 {
   using namespace gnufft;
-  PlanView v;
-  if (!plan_view(plan, &v) || !kspace || !grid)
-  {
-    set_last_error("NULL argument");
-    return GNUFFT_ERROR_INVALID_ARGUMENT;
-  }
-  if (n_coils == 0 || (v.sens_coils && n_coils != v.sens_coils))
-  {
-    set_last_error("n_coils must be positive and match the sensitivity maps");
-    return GNUFFT_ERROR_INVALID_ARGUMENT;
-  }
-  const int cg = spmm_coil_group((int)n_coils);
-  const size_t CP = ((size_t)n_coils + cg - 1) / cg * cg;
-  const size_t need = (size_t)v.M * CP;
-  if (need > kScratchElems)
-  {
-    set_last_error("no-allocation adjoint: samples x coil lanes (" +
-                   std::to_string(v.M) + " x " + std::to_string(CP) + " = " +
-                   std::to_string(need * sizeof(float2)) +
-                   " bytes) exceed the fixed " +
-                   std::to_string(kScratchBytes) + "-byte staging area");
-    return GNUFFT_ERROR_INVALID_ARGUMENT;
-  }
   int prev = -1;
-  cudaGetDevice(&prev);
+  gnufft_status st = GNUFFT_SUCCESS;
   try
   {
+    PlanView v;
+    if (!plan_view(plan, &v) || !kspace || !grid)
+      throw Error(kInvalidArgument, "NULL argument");
+    if (n_coils == 0 || (v.sens_coils && n_coils != v.sens_coils))
+      throw Error(kInvalidArgument,
+                  "n_coils must be positive and match the sensitivity maps");
+    const int cg = spmm_coil_group((int)n_coils);
+    const size_t CP = ((size_t)n_coils + cg - 1) / cg * cg;
+    const size_t need = (size_t)v.M * CP;
+    if (need > kScratchElems)
+      throw Error(kInvalidArgument,
+                  "no-allocation adjoint: samples x coil lanes (" +
+                      std::to_string(v.M) + " x " + std::to_string(CP) +
+                      " = " + std::to_string(need * sizeof(float2)) +
+                      " bytes) exceed the fixed " +
+                      std::to_string(kScratchBytes) +
+                      "-byte staging area");
+    cudaGetDevice(&prev);
     GN_CUDA(cudaSetDevice(v.device));
-    float2 *ks = scratch_address(v.device);
+    float2 *ks = scratch_address();
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     // Every one of the M x CP staged entries is written (coil lanes beyond
     // n_coils as zeros), so nothing left from an earlier call is read.
@@ -104,11 +90,14 @@ extern "C" gnufft_status gnufft_adjoint_convolution_noalloc(gnufft_plan *plan,
   catch (const Error &e)
   {
     set_last_error(e.what());
-    if (prev >= 0)
-      cudaSetDevice(prev);
-    return (gnufft_status)e.status;
+    st = (gnufft_status)e.status;
+  }
+  catch (const std::exception &e)
+  {
+    set_last_error(e.what());
+    st = GNUFFT_ERROR_INTERNAL;
   }
   if (prev >= 0)
     cudaSetDevice(prev);
-  return GNUFFT_SUCCESS;
+  return st;
 }

@@ -32,6 +32,7 @@
 #include "geometry.hpp"
 #include "gridding.cuh"
 #include "planview.hpp"
+#include "tma.cuh"
 #include "trajgrad.cuh"
 
 using namespace gnufft;
@@ -78,6 +79,7 @@ struct gnufft_plan
   bool fwd_signs = false;
   int *copy_err_h = nullptr;  // set by a tile copy that timed out (mapped)
   int *copy_err_d = nullptr;
+  long long copy_polls = tma::kMbarSpin;  // first wait of a tile copy
   // TEXTURE operators: the lookup table as a filtered texture
   cudaArray_t lut_array = nullptr;
   cudaTextureObject_t lut_tex = 0;
@@ -587,9 +589,20 @@ void check_coils(const gnufft_plan &p, uint32_t C)
                 "n_coils differs from the sensitivity map channels");
 }
 
+// The error flag and first-wait bound of the plan's tile copies.
+tma::CopyWait copy_wait(const gnufft_plan &p)
+{
+  tma::CopyWait cw;
+  cw.err = p.copy_err_d;
+  cw.polls = p.copy_polls;
+  return cw;
+}
+
 // Root tables (once) and grow-only scratch of the pruned transforms.
-// A tile copy of an earlier call that did not complete within its bounded
-// wait set the mapped flag: report it (once) instead of computing on.
+// A tile copy that did not complete within its bounded wait set the mapped
+// flag: report it (once).  Checked at the start of every call (copies of an
+// earlier device call) and at the end of the synchronous host calls (their
+// own copies).
 void check_copy_err(gnufft_plan &p)
 {
   if (p.copy_err_h && *(volatile int *)p.copy_err_h)
@@ -666,7 +679,7 @@ void adjoint_batched(gnufft_plan &p, const float2 *k, float2 *img, uint32_t C,
           grid, p.deapo.as<float>(),
           stage == GNUFFT_DEAPODIZATION ? sens : nullptr, g, (int)C,
           stage == GNUFFT_FFT ? 1 : 2, accumulate, root_ptrs(p).data(),
-          p.fft_b.as<float2>(), p.fft_a.as<float2>(), img, s, p.copy_err_d);
+          p.fft_b.as<float2>(), p.fft_a.as<float2>(), img, s, copy_wait(p));
       p.launches += g.dim - 1;
       p.mark(5, s);
       p.mark(6, s);
@@ -743,7 +756,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
     launch_pruned_forward(img, sens, p.deapo.as<float>(), g, (int)C,
                           root_ptrs(p).data(), p.fft_a.as<float2>(),
                           p.fft_b.as<float2>(), grid, s,
-                          p.zrange.as<uint2>(), p.copy_err_d, paired);
+                          p.zrange.as<uint2>(), copy_wait(p), paired);
     p.launches += g.dim;
     p.mark(5, s);
     p.mark(2, s);
@@ -752,7 +765,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
             p.fwd_items.as<FwdItem>(), p.n_fwd_items,
             p.traj_sorted.as<float>(), p.di.as<uint32_t>(),
             p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
-            p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, p.copy_err_d, s,
+            p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, copy_wait(p), s,
             p.fwd_tile_coils, paired))
       launch_forward_interp(
           p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
@@ -791,7 +804,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
           p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
           p.di.as<uint32_t>(),
           p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
-          p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, p.copy_err_d, s,
+          p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, copy_wait(p), s,
           p.fwd_tile_coils, false))
     launch_forward_interp(
         p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
@@ -1095,6 +1108,21 @@ gnufft_status gnufft_set_sens_device(gnufft_plan *p, const void *sens,
   });
 }
 
+gnufft_status gnufft_set_copy_wait(gnufft_plan *p, int64_t polls)
+{
+  if (!p)
+    return (gnufft_status)fail(kInvalidArgument, "plan is NULL");
+  p->copy_polls = polls < 0 ? tma::kMbarSpin : (long long)polls;
+  return GNUFFT_SUCCESS;
+}
+
+gnufft_status gnufft_plan_check(gnufft_plan *p)
+{
+  if (!p)
+    return (gnufft_status)fail(kInvalidArgument, "plan is NULL");
+  return guarded([&] { check_copy_err(*p); });
+}
+
 gnufft_status gnufft_set_timing(gnufft_plan *p, int enable)
 {
   if (!p)
@@ -1214,6 +1242,7 @@ gnufft_status gnufft_adjoint_host(gnufft_plan *p, const void *kspace,
                             cudaMemcpyDeviceToHost, s));
     GN_CUDA(cudaStreamSynchronize(s));
     collect_times(*p, s);
+    check_copy_err(*p);  // this call's own tile copies
   });
 }
 
@@ -1252,6 +1281,7 @@ gnufft_status gnufft_forward_host(gnufft_plan *p, const void *image,
                             cudaMemcpyDeviceToHost, s));
     GN_CUDA(cudaStreamSynchronize(s));
     collect_times(*p, s);
+    check_copy_err(*p);  // this call's own tile copies
   });
 }
 

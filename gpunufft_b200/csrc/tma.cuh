@@ -41,6 +41,16 @@ inline EncodeTiledFn encode_fn()
 // by then is reported through the caller's error flag.
 constexpr long long kMbarSpin = 1LL << 22;
 
+// Error reporting of the tile copies of one launch: `err` (a mapped host
+// flag) is set when a block's wait for a copy gives up after `polls` polls
+// (kMbarSpin by default); the waits a block makes before returning, for its
+// copies still in flight, always use kMbarSpin.
+struct CopyWait
+{
+  int *err = nullptr;
+  long long polls = kMbarSpin;
+};
+
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -75,13 +85,14 @@ __device__ __forceinline__ void fence_proxy_async()
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
 
-// Waits (at most kMbarSpin polls) for the phase with the given parity to
+// Waits (at most `polls` polls) for the phase with the given parity to
 // complete; false if it did not.
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar,
-                                                  uint32_t parity)
+                                                  uint32_t parity,
+                                                  long long polls = kMbarSpin)
 {
   uint32_t done = 0;
-  for (long long i = 0; i < kMbarSpin && !done; ++i)
+  for (long long i = 0; i < polls && !done; ++i)
     asm volatile(
         "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, "
         "[%1], %2; selp.u32 %0, 1, 0, p; }"

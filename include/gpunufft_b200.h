@@ -234,11 +234,11 @@ GNUFFT_API gnufft_status gnufft_forward_device(gnufft_plan *plan, const void *im
  * n_samples x coil lanes x 8 bytes must fit in it (coil lanes: n_coils
  * rounded up to 1, 2, 4, 8, 16 or a multiple of 32); larger requests are
  * rejected with GNUFFT_ERROR_INVALID_ARGUMENT.  kspace and grid are device
- * buffers; the call is ordered on `stream`.  The first call on a device
- * looks up the array's device address (set-up, once per device); make that
- * first call before any stream capture.  All calls on a device share the
- * array: calls that overlap on the GPU race and must be serialised by the
- * caller. */
+ * buffers; the call is ordered on `stream`.  Every call looks up the
+ * array's device address on the plan's device (the first call on a device
+ * also loads the library's device code there); make that first call before
+ * any stream capture.  All calls on a device share the array: calls that
+ * overlap on the GPU race and must be serialised by the caller. */
 #define GNUFFT_NOALLOC_SCRATCH_BYTES ((size_t)16 << 20)
 GNUFFT_API gnufft_status gnufft_adjoint_convolution_noalloc(
     gnufft_plan *plan, const void *kspace, void *grid, uint32_t n_coils,
@@ -268,6 +268,21 @@ typedef struct gnufft_stage_times {
   uint32_t launches;  /* kernels of this library launched by the call */
 } gnufft_stage_times;
 GNUFFT_API gnufft_status gnufft_set_timing(gnufft_plan *plan, int enable);
+
+/* Tile copies of this library's kernels complete on a bounded wait: a copy
+ * that has not completed after the wait's polls sets a flag, the block
+ * stops (after a bounded wait for its copies in flight) and the call
+ * reports GNUFFT_ERROR_CUDA ("a tile copy did not complete within its
+ * wait") -- the host calls at their end, a device call at the plan's next
+ * call or at gnufft_plan_check after the caller synchronised its stream.
+ * No counterpart in the upstream (which waits without bound).
+ * gnufft_set_copy_wait sets the polls of each block's first wait for a copy
+ * (negative: the default, about 4 million); a small value exercises the
+ * failure path (0 gives up at once).  gnufft_plan_check returns and clears
+ * a pending copy failure of the plan. */
+GNUFFT_API gnufft_status gnufft_set_copy_wait(gnufft_plan *plan,
+                                              int64_t polls);
+GNUFFT_API gnufft_status gnufft_plan_check(gnufft_plan *plan);
 GNUFFT_API gnufft_status gnufft_get_stage_times(const gnufft_plan *plan,
                                      gnufft_stage_times *times);
 

@@ -170,3 +170,28 @@ def test_data_consistency_step_256_16coil():
     with torch.no_grad():
         ref = plan.adjoint(2 * (plan.forward(x) - y))
     assert rel_l2(x.grad.cpu().numpy(), ref.cpu().numpy()) < 1e-5
+
+
+def test_plan_reuse_follows_the_trajectory():
+    """The module rebuilds its plan only when the trajectory changes: the
+    same tensor (or an equal one) reuses it, an in-place update or a new
+    trajectory builds a new one, and results follow the trajectory."""
+    import torch
+
+    from gpunufft_b200.autograd import NUFFT
+    traj = torch.from_numpy(radial_2d(16, 32)).cuda()
+    op = NUFFT((16, 16))
+    x = torch.randn(1, 16, 16, dtype=torch.complex64, device="cuda")
+    y0 = op(x, traj)
+    p0 = op._plan
+    assert op(x, traj) is not None and op._plan is p0
+    assert op(x, traj.clone()) is not None and op._plan is p0
+    with torch.no_grad():
+        traj[0, 3] += 0.01
+    y1 = op(x, traj)
+    assert op._plan is not p0
+    assert rel_l2(y1.cpu().numpy(), y0.cpu().numpy()) > 1e-6
+    p1 = op._plan
+    fresh = NUFFT((16, 16))
+    assert rel_l2(fresh(x, traj).cpu().numpy(), y1.cpu().numpy()) < 1e-6
+    assert op(x, traj) is not None and op._plan is p1

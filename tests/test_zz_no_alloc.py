@@ -7,8 +7,10 @@ budget, callers that cannot take the synchronisation of cudaMalloc /
 cudaFree).  It stages its scratch in a fixed array inside the library.
 This test calls it through the C ABI twice in a row -- the second call with
 other data, so stale contents of the shared array would show -- and checks
-both results against ``gnufft_adjoint_device`` with GNUFFT_CONVOLUTION.
-This file is collected last on purpose.
+both results against ``gnufft_adjoint_device`` with GNUFFT_CONVOLUTION, and
+that the device's free memory (cudaMemGetInfo) is the same before and after
+a warm call.  A request that fills the staging area exactly is accepted; one
+beyond it is rejected.  This file is collected last on purpose.
 """
 import ctypes
 
@@ -38,17 +40,45 @@ def test_noalloc_matches_regular_adjoint_twice(dims, traj_fn, n_coils, dens):
     plan = G.Plan(traj, dims, 3, 8, 2.0, w, None, G.BALANCED)
     L = _capi.lib()
     stream = torch.cuda.current_stream().cuda_stream
+    ks = [torch.from_numpy(cplx(rng, n_coils, M)).cuda() for _ in range(2)]
+    outs = [torch.empty((n_coils,) + plan.grid_shape, dtype=torch.complex64,
+                        device="cuda") for _ in range(2)]
+    exps = [plan.adjoint(k, G.CONVOLUTION) for k in ks]
+    torch.cuda.synchronize()
+    free = []
     for call in range(2):
-        k = torch.from_numpy(cplx(rng, n_coils, M)).cuda()
-        out = torch.empty((n_coils,) + plan.grid_shape,
-                          dtype=torch.complex64, device="cuda")
+        free.append(torch.cuda.mem_get_info()[0])
         _capi.check(L.gnufft_adjoint_convolution_noalloc(
-            plan._h, ctypes.c_void_p(k.data_ptr()),
-            ctypes.c_void_p(out.data_ptr()), n_coils,
+            plan._h, ctypes.c_void_p(ks[call].data_ptr()),
+            ctypes.c_void_p(outs[call].data_ptr()), n_coils,
             ctypes.c_void_p(stream)))
-        exp = plan.adjoint(k, G.CONVOLUTION)
         torch.cuda.synchronize()
-        assert rel_l2(out.cpu().numpy(), exp.cpu().numpy()) < TOL, call
+        assert rel_l2(outs[call].cpu().numpy(),
+                      exps[call].cpu().numpy()) < TOL, call
+    # the warm call allocated nothing on the device
+    assert torch.cuda.mem_get_info()[0] == free[1]
+
+
+def test_noalloc_accepts_a_request_that_fills_its_staging_area():
+    torch = pytest.importorskip("torch")
+    import gpunufft_b200 as G
+    from gpunufft_b200 import _capi
+
+    rng = np.random.default_rng(9)
+    traj = kooshball_3d(512, 64)  # 32768 samples
+    plan = G.Plan(traj, (16, 16, 16), 3, 8, 2.0, None, None, G.BALANCED)
+    n_coils = 64  # 64 coil lanes x 32768 samples x 8 bytes = 16 MiB exactly
+    assert traj.shape[1] * n_coils * 8 == _capi.NOALLOC_SCRATCH_BYTES
+    k = torch.from_numpy(cplx(rng, n_coils, traj.shape[1])).cuda()
+    out = torch.empty((n_coils,) + plan.grid_shape, dtype=torch.complex64,
+                      device="cuda")
+    _capi.check(_capi.lib().gnufft_adjoint_convolution_noalloc(
+        plan._h, ctypes.c_void_p(k.data_ptr()),
+        ctypes.c_void_p(out.data_ptr()), n_coils,
+        ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    exp = plan.adjoint(k, G.CONVOLUTION)
+    torch.cuda.synchronize()
+    assert rel_l2(out.cpu().numpy(), exp.cpu().numpy()) < TOL
 
 
 def test_noalloc_rejects_requests_beyond_its_staging_area():
