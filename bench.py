@@ -256,24 +256,55 @@ def reference_gpu(inp, steps):
     from oracle import ref
     note = ("upstream BALANCED operator built from its sources for sm_100a "
             "(textures off); host arrays per call as its API takes them; "
-            "wall clock")
+            "CUDA events on the default stream (value) and wall clock")
     if not ref.available():
         return {"value": None, "unit": UNIT, "note": note + ": not built"}
     op = ref.RefGpuOperator(inp["traj"], inp["dims"], inp["C"], inp["kw"],
                             inp["sw"], inp["osf"], sens=inp["maps"],
                             balance=True)
     try:
-        op.forward(inp["x"])
-        op.adjoint(inp["k"])
-        t0 = time.perf_counter()
-        for _ in range(steps):
-            op.forward(inp["x"])
-            op.adjoint(inp["k"])
-        dt = time.perf_counter() - t0
+        ms, wall_ms = timed_steps(lambda: (op.forward(inp["x"]),
+                                           op.adjoint(inp["k"])), steps)
     finally:
         op.close()
-    return {"value": steps / dt, "unit": UNIT, "steps": steps,
-            "ms_per_step": dt / steps * 1e3, "note": note}
+    return {"value": 1e3 / ms, "unit": UNIT, "steps": steps,
+            "ms_per_step": ms, "wall_value": 1e3 / wall_ms,
+            "wall_ms_per_step": wall_ms, "note": note}
+
+
+def timed_steps(fn, steps, warmup=1):
+    """(device ms per step, wall ms per step) of fn after `warmup` calls:
+    CUDA events on the current (legacy default) stream, which every call
+    here is ordered on or synchronises with, and the host clock."""
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t0 = time.perf_counter()
+    e0.record()
+    for _ in range(steps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    wall = (time.perf_counter() - t0) * 1e3 / steps
+    return e0.elapsed_time(e1) / steps, wall
+
+
+def plan_creation_ms(make, reps=3):
+    """Median wall ms of creating (and synchronising) a plan; the plan is
+    destroyed after each creation."""
+    import torch
+    ts = []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p = make()
+        torch.cuda.synchronize()
+        ts.append((time.perf_counter() - t0) * 1e3)
+        p.close()
+    return statistics.median(ts)
 
 
 def workload_label(name):
@@ -299,15 +330,21 @@ def peaks():
 
 
 def profile_traffic(name, kernel):
-    """DRAM bytes (read + write) per launch of ``kernel`` on workload
-    ``name`` from the committed ncu summary, if one exists."""
+    """(DRAM bytes read + written per launch of ``kernel`` on workload
+    ``name``, where the figure comes from) from the committed ncu summary;
+    (None, None) without one."""
     p = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(p) as f:
             d = json.load(f)
-        return d[name][kernel]["dram_bytes_per_launch"]
+        e = d[name][kernel]
+        src = e.get("scaled_from")
+        how = (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of the "
+               f"{src} capture, scaled by the units processed" if src else
+               "ncu dram__bytes_read.sum + dram__bytes_write.sum")
+        return e["dram_bytes_per_launch"], how
     except Exception:
-        return None
+        return None, None
 
 
 def reduce_over_ranks(value, dist, device, op="max"):
@@ -420,12 +457,18 @@ def run_gpu_arm(args, rank, world, dist):
     rooflines = []
     for kname, (what, kms, nbytes) in kernels.items():
         ach = nbytes / (kms * 1e-3) / 1e9
+        traffic, tsrc = profile_traffic(args.workload, kname)
+        # the gridding bytes as the survey counts them for either direction:
+        # k-space, coordinates and the oversampled grid once each
+        sach = gbytes / (kms * 1e-3) / 1e9
         rooflines.append({
             "kernel": kname, "what": what, "bound": "hbm", "achieved": ach,
             "peak": peak, "peak_source": src, "unit": "GB/s",
-            "frac": ach / peak, "traffic": profile_traffic(args.workload,
-                                                           kname),
-            "algorithmic_bytes": nbytes, "launch_ms": kms})
+            "frac": ach / peak, "traffic": traffic,
+            "traffic_source": tsrc,
+            "algorithmic_bytes": nbytes,
+            "gridding_bytes": gbytes, "gridding_achieved": sach,
+            "gridding_frac": sach / peak, "launch_ms": kms})
     # the dominant one of this library's kernels (longest per step)
     roofline = max(rooflines, key=lambda r: r["launch_ms"])
 
@@ -489,22 +532,53 @@ def run_gpu_arm(args, rank, world, dist):
 
     # plain per-call operator (the upstream's flow: one coil per pass, maps
     # copied per coil per call, a synchronisation per coil)
-    plain_value = None
+    plain = {"value": None, "unit": UNIT, "steps": args.plain_steps}
     if args.plain_steps > 0:
         plan_p = G.Plan(inp["traj"], dims, inp["kw"], inp["sw"], inp["osf"],
                         None, inp["maps"], G.BALANCED, plain=True, device=dev)
-        plan_p.forward(x_d)
-        plan_p.adjoint(k_d)
-        torch.cuda.synchronize()
-        p0 = time.perf_counter()
-        for _ in range(args.plain_steps):
-            plan_p.forward(x_d)
-            plan_p.adjoint(k_d)
-        torch.cuda.synchronize()
-        plain_value = args.plain_steps / (time.perf_counter() - p0)
+        pms, pwall = timed_steps(lambda: (plan_p.forward(x_d),
+                                          plan_p.adjoint(k_d)),
+                                 args.plain_steps)
         plan_p.close()
-        plain_value = reduce_over_ranks(plain_value, dist, dev,
-                                        "min") * world
+        pms = reduce_over_ranks(pms, dist, dev)
+        plain.update(value=world * 1e3 / pms, ms_per_step=pms,
+                     wall_value=world * 1e3 / pwall, wall_ms_per_step=pwall,
+                     batched_over_plain=value / (world * 1e3 / pms))
+    # the host-array API (gnufft_forward_host / gnufft_adjoint_host: the
+    # counterpart of the upstream's performForwardGpuNUFFT /
+    # performGpuNUFFTAdj on host Arrays): host buffers in and out,
+    # synchronous per call
+    host_api = None
+    if args.host_steps > 0:
+        xh_np = inp["x"]
+        kh_np = inp["k"]
+        hms, hwall = timed_steps(lambda: (plan.forward(xh_np),
+                                          plan.adjoint(kh_np)),
+                                 args.host_steps)
+        hms = reduce_over_ranks(hms, dist, dev)
+        host_api = {"value": world * 1e3 / hms, "unit": UNIT,
+                    "steps": args.host_steps, "ms_per_step": hms,
+                    "wall_value": world * 1e3 / hwall,
+                    "wall_ms_per_step": hwall,
+                    "note": "Plan.forward / adjoint on NumPy arrays "
+                            "(pageable host memory), copies inside each "
+                            "call"}
+    # plan creation (sector binning, sort, tables, interpolation matrix,
+    # deapodization) for this workload and for the 2-D 256^2 x 16-coil
+    # radial 402 x 512 workload of the differentiable operator
+    creation = {}
+    if rank == 0 and args.plan_timing:
+        creation["workload_ms"] = plan_creation_ms(
+            lambda: G.Plan(inp["traj"], dims, inp["kw"], inp["sw"],
+                           inp["osf"], None, inp["maps"], G.BALANCED,
+                           device=dev))
+        tr4 = radial2d(402, 512)
+        rng4 = np.random.default_rng(4)
+        m4 = (rng4.standard_normal((16, 256, 256)) + 1j *
+              rng4.standard_normal((16, 256, 256))).astype(np.complex64)
+        creation["2d256_16coil_radial402x512_ms"] = plan_creation_ms(
+            lambda: G.Plan(tr4, (256, 256), 3, 8, 2.0, None, m4, G.BALANCED,
+                           device=dev))
 
     # the upstream library's own GPU operator, built from its sources for
     # sm_100a (oracle/_ref), on the same inputs through its host-array API
@@ -514,6 +588,10 @@ def run_gpu_arm(args, rank, world, dist):
     if args.ref_gpu_steps > 0:
         ref_gpu = reference_gpu(inp, args.ref_gpu_steps)
 
+    batched = None
+    if args.batch_instances > 0 and rank == 0:
+        batched = batch_run(dev, args.steps, args.warmup,
+                            n_instances=args.batch_instances)
     served = None
     if args.serve_requests > 0:
         served = serving_run(dev, args.serve_requests, seed=rank)
@@ -562,12 +640,12 @@ def run_gpu_arm(args, rank, world, dist):
                             ("prepare_ms", "gridding_ms", "fft_ms",
                              "finish_ms")},
             },
-            "plain": {"value": plain_value, "unit": UNIT,
-                      "steps": args.plain_steps,
-                      "batched_over_plain": (value / plain_value
-                                             if plain_value else None)},
+            "plain": plain,
+            "host_api": host_api,
+            "plan_creation_ms": creation,
             "reference_gpu": ref_gpu,
             "served": served,
+            "batched_uneven": batched,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -581,10 +659,12 @@ def run_gpu_arm(args, rank, world, dist):
 def serving_run(dev, n_requests, seed=0):
     """Poisson arrivals (mean 50 requests/s) of mixed CG-SENSE requests, 10
     iterations each: 2-D radial/spiral 128-384^2 with 1-32 coils and
-    20k-400k samples, or (one in eight) 3-D kooshball 96^3-128^3 with 8-16
-    coils and 0.5M-1M samples.  Trajectories come from a pool of ten (so
-    operators are reused); maps per (size, coils).  Returns the server's
-    statistics."""
+    20k-400k samples, or 3-D kooshball 96^3-160^3 with 8-32 coils and
+    0.5M-3M samples (two of the ten trajectories of the pool, so about one
+    request in five).  Operators are reused per trajectory; maps per (size,
+    coils).  Returns the server's statistics: cold (first pass, operators
+    built on demand) and warm (the same arrivals again, operators
+    resident) latencies side by side."""
     from gpunufft_b200.batch import spiral_trajectory
     from gpunufft_b200.serving import Request, Server
     rng = np.random.default_rng(seed)
@@ -599,8 +679,8 @@ def serving_run(dev, n_requests, seed=0):
                 traj = spiral_trajectory(int(rng.integers(8, 49)), M, rng)
             pool.append(((size, size), traj))
         else:
-            size = int(rng.choice([96, 128]))
-            M = int(rng.integers(500_000, 1_000_001))
+            size = int(rng.choice([96, 128, 160]))
+            M = int(rng.integers(500_000, 3_000_001))
             nr = 2 * size
             pool.append(((size,) * 3, kooshball(max(1, M // nr), nr)))
     import copy
@@ -631,7 +711,7 @@ def serving_run(dev, n_requests, seed=0):
     for i in range(n_requests):
         t += rng.exponential(1 / 50.0)
         dims, traj = pool[int(rng.integers(0, 10))]
-        C = (int(rng.integers(8, 17)) if len(dims) == 3 else
+        C = (int(rng.integers(8, 33)) if len(dims) == 3 else
              int(rng.integers(1, 33)))
         M = traj.shape[1]
         k = (rng.standard_normal((C, M), dtype=np.float32) + 1j *
@@ -652,29 +732,37 @@ def serving_run(dev, n_requests, seed=0):
         st = srv.stats()
     finally:
         srv.close()
-    st["cold_p50_ms"] = cold["p50_ms"]
-    st["cold_p99_ms"] = cold["p99_ms"]
-    st["workload"] = (f"{n_requests} CG-SENSE requests x 10 iterations, "
-                      f"Poisson 50/s, 2-D 128-384^2 / 3-D 96-128^3 mix; "
-                      f"p50/p99 of the second pass (operators resident), "
-                      f"cold = first pass")
-    return st
+    out = {
+        "cold": {k: cold[k] for k in ("p50_ms", "p99_ms", "throughput_rps",
+                                      "plan_cache_misses")},
+        "warm": {k: st[k] for k in ("p50_ms", "p99_ms", "throughput_rps",
+                                    "plan_cache_hits")},
+        "requests": st["requests"], "max_concurrent": st["max_concurrent"],
+        "peak_hbm_gb": max(st["peak_hbm_gb"], cold["peak_hbm_gb"]),
+        "peak_live_gb": max(st["peak_live_gb"], cold["peak_live_gb"]),
+        "peak_admitted_gb": max(st["peak_admitted_gb"],
+                                cold["peak_admitted_gb"]),
+        "workload": (f"{n_requests} CG-SENSE requests x 10 iterations, "
+                     f"Poisson 50/s, 2-D 128-384^2 1-32 coils 20k-400k "
+                     f"samples / 3-D 96-160^3 8-32 coils 0.5M-3M samples; "
+                     f"cold = first pass (operators built on demand), warm "
+                     f"= the same arrivals again (operators resident)")}
+    return out
 
 
-def run_batch_arm(args, rank, world):
-    """64 uneven 2-D spiral operators (image 96-320^2, 8-32 coils, 10k-120k
-    samples, osf 1.25-2, kernel width 3-5; sector width and forward tile
-    from the autotuner): fwd + adj of every instance per step, replayed
-    from one CUDA graph, against the plain per-instance loop."""
+def batch_run(dev, steps, warmup, seed=0, n_instances=64):
+    """``n_instances`` uneven 2-D spiral operators (image 96-320^2, 8-32
+    coils, 10k-120k samples, osf 1.25-2, kernel width 3-5; sector width and
+    forward tile from the autotuner): fwd + adj of every instance per step,
+    replayed from one CUDA graph, against the plain per-instance loop.
+    Device-timed ms per step of both."""
     import torch
 
     import gpunufft_b200 as G
     from gpunufft_b200.batch import BatchedOperator, autotune, \
         spiral_instances
-    dev = int(os.environ.get("LOCAL_RANK", 0))
-    torch.cuda.set_device(dev)
-    specs = spiral_instances(64, seed=rank)
-    rng = np.random.default_rng(rank)
+    specs = spiral_instances(n_instances, seed=seed)
+    rng = np.random.default_rng(seed)
     plans, coils, tuned = [], [], []
     t0 = time.perf_counter()
     for s in specs:
@@ -706,47 +794,51 @@ def run_batch_arm(args, rank, world):
         x.copy_(torch.randn_like(x))
     for k in bo.k_in:
         k.copy_(torch.randn_like(k))
-
-    def timed(fn):
-        for _ in range(args.warmup):
-            fn()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(args.steps):
-            fn()
-        e1.record()
-        torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / args.steps
-
-    ms_graph = timed(lambda: (bo.replay("forward"), bo.replay("adjoint")))
-    ms_plain = timed(lambda: (bo.plain("forward"), bo.plain("adjoint")))
+    ms_graph, _ = timed_steps(lambda: (bo.replay("forward"),
+                                       bo.replay("adjoint")), steps,
+                              max(warmup, 1))
+    ms_plain, _ = timed_steps(lambda: (bo.plain("forward"),
+                                       bo.plain("adjoint")), steps,
+                              max(warmup, 1))
+    sw_hist = {}
+    for sw, tc in tuned:
+        key = f"sw{sw}/tile{tc or 'auto'}"
+        sw_hist[key] = sw_hist.get(key, 0) + 1
+    for p in plans:
+        p.close()
     n = len(plans)
+    return {"value": n / (ms_graph * 1e-3), "unit": "instances/s",
+            "ms_per_step": ms_graph, "instances": n,
+            "plain": {"value": n / (ms_plain * 1e-3),
+                      "ms_per_step": ms_plain},
+            "graph_over_plain": ms_plain / ms_graph,
+            "autotune": {"seconds": tune_s, "choices": sw_hist},
+            "workload": f"{n} variable-density 2-D spirals, image 96-320^2, "
+                        "8-32 coils, 10k-120k samples, osf 1.25-2, kw 3-5, "
+                        "coil maps; one step = forward + adjoint of every "
+                        "instance"}
+
+
+def run_batch_arm(args, rank, world):
+    """The uneven spiral batch as the benchmark's workload."""
+    import torch
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    b = batch_run(dev, args.steps, args.warmup, seed=rank)
     if rank == 0:
-        sw_hist = {}
-        for sw, tc in tuned:
-            sw_hist[f"sw{sw}/tile{tc or 'auto'}"] = \
-                sw_hist.get(f"sw{sw}/tile{tc or 'auto'}", 0) + 1
         print(json.dumps({
             "metric": "uneven batch: instance fwd+adj/s, one CUDA graph vs "
                       "plain per-instance loop",
-            "value": world * n / (ms_graph * 1e-3), "unit": "instances/s",
+            "value": world * b["value"], "unit": "instances/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_graph, "higher_is_better": True,
+            "ms_per_step": b["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": "64 variable-density 2-D spirals, image "
-                                   "96-320^2, 8-32 coils, 10k-120k samples, "
-                                   "osf 1.25-2, kw 3-5, coil maps",
-                       "instances": n},
-            "plain": {"value": world * n / (ms_plain * 1e-3),
-                      "ms_per_step": ms_plain,
-                      "graph_over_plain": ms_plain / ms_graph},
-            "autotune": {"seconds": tune_s, "choices": sw_hist},
+            "config": {"workload": b["workload"],
+                       "instances": b["instances"]},
+            "plain": b["plain"], "graph_over_plain": b["graph_over_plain"],
+            "autotune": b["autotune"],
         }), flush=True)
-    for p in plans:
-        p.close()
 
 
 def main():
@@ -757,11 +849,19 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="3d128x32",
                     choices=list(WORKLOADS) + ["spirals64"])
-    ap.add_argument("--plain-steps", type=int, default=2)
+    ap.add_argument("--plain-steps", type=int, default=5)
+    ap.add_argument("--host-steps", type=int, default=5,
+                    help="steps of the host-array API arm (0: skip)")
+    ap.add_argument("--batch-instances", type=int, default=64,
+                    help="instances of the uneven spiral batch reported "
+                         "beside the workload (0: skip)")
+    ap.add_argument("--no-plan-timing", dest="plan_timing",
+                    action="store_false",
+                    help="skip the plan-creation timings")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=40,
                     help="requests of the serving run (0: skip)")
-    ap.add_argument("--ref-gpu-steps", type=int, default=2,
+    ap.add_argument("--ref-gpu-steps", type=int, default=5,
                     help="steps of the upstream GPU operator (0: skip)")
     args = ap.parse_args()
 

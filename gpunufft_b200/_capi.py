@@ -47,6 +47,7 @@ EXPORTED = (
     "gnufft_adjoint_convolution_noalloc",
     "gnufft_traj_grad_device", "gnufft_set_sens_device",
     "gnufft_set_copy_wait", "gnufft_plan_check",
+    "gnufft_set_memory_limit", "gnufft_call_scratch_bytes",
 )
 
 
@@ -138,6 +139,11 @@ def lib() -> ctypes.CDLL:
     L.gnufft_traj_grad_device.restype = st
     L.gnufft_traj_grad_device.argtypes = [_P, _P, _P, _U, _P, _P]
     L.gnufft_set_timing.restype = st
+    L.gnufft_set_memory_limit.restype = ctypes.c_int
+    L.gnufft_set_memory_limit.argtypes = [_P, ctypes.c_uint64]
+    L.gnufft_call_scratch_bytes.restype = ctypes.c_int
+    L.gnufft_call_scratch_bytes.argtypes = [_P, _U,
+                                            ctypes.POINTER(ctypes.c_uint64)]
     L.gnufft_set_copy_wait.restype = ctypes.c_int
     L.gnufft_set_copy_wait.argtypes = [_P, ctypes.c_int64]
     L.gnufft_plan_check.restype = ctypes.c_int

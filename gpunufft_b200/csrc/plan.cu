@@ -80,6 +80,7 @@ struct gnufft_plan
   int *copy_err_h = nullptr;  // set by a tile copy that timed out (mapped)
   int *copy_err_d = nullptr;
   long long copy_polls = tma::kMbarSpin;  // first wait of a tile copy
+  size_t mem_limit = 0;  // scratch cap of a call (0: the free memory)
   // TEXTURE operators: the lookup table as a filtered texture
   cudaArray_t lut_array = nullptr;
   cudaTextureObject_t lut_tex = 0;
@@ -847,6 +848,99 @@ void traj_grad(gnufft_plan &p, const float2 *img, const float2 *u, uint32_t C,
   p.launches += 3;
 }
 
+// Device scratch the plan's buffers grow to for calls with C coils
+// (forward and adjoint share them): the sorted k-space lanes, the grid and
+// the transform passes' buffers (cuFFT's work area counted as one grid).
+size_t call_scratch_bytes(const gnufft_plan &p, uint32_t C)
+{
+  const Geo &g = p.g;
+  const size_t G = (size_t)g.grid_count, f2 = sizeof(float2);
+  const size_t cg = (size_t)spmm_coil_group((int)C);
+  const size_t CP = (C + cg - 1) / cg * cg;
+  size_t b = (size_t)p.M * CP * f2 + (size_t)(C + 1) / 2 * 2 * G * f2;
+  if (p.pruned)
+    b += (pruned_scratch_a(g, (int)C) +
+          std::max(pruned_scratch_b(g, (int)C),
+                   pruned_scratch_xfirst(g, (int)C))) *
+         f2;
+  else
+    b += (size_t)C * G * f2;
+  return b;
+}
+
+size_t held_scratch_bytes(const gnufft_plan &p)
+{
+  return p.ks.bytes() + p.grid.bytes() + p.fft_a.bytes() + p.fft_b.bytes();
+}
+
+// Coils per pass so that a pass's scratch fits the plan's memory limit, or
+// else the device memory free now (plus what the plan's scratch holds
+// already, minus a margin) -- the upstream's concurrent coil count
+// (computePossibleConcurrentCoilCount, gpuNUFFT_operator.cpp:327-368),
+// for 2-D and 3-D alike.  At least one coil.
+uint32_t coils_per_pass(const gnufft_plan &p, uint32_t C)
+{
+  size_t limit = p.mem_limit;
+  if (!limit)
+  {
+    size_t free_b = 0, total_b = 0;
+    GN_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t margin = (size_t)256 << 20;
+    const size_t avail = free_b + held_scratch_bytes(p);
+    limit = avail > margin ? avail - margin : 0;
+  }
+  if (call_scratch_bytes(p, C) <= limit)
+    return C;
+  uint32_t lo = 1, hi = C;  // largest c with scratch(c) <= limit
+  while (lo < hi)
+  {
+    const uint32_t mid = (lo + hi + 1) / 2;
+    if (call_scratch_bytes(p, mid) <= limit)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+// A batched call in coil passes of at most coils_per_pass coils: k-space,
+// maps and per-coil outputs advance by the pass's first coil; the
+// coil-combined image (maps, DEAPODIZATION) is summed over the passes.
+void adjoint_chunked(gnufft_plan &p, const float2 *k, float2 *img,
+                     uint32_t C, int stage, cudaStream_t s)
+{
+  const uint32_t step = coils_per_pass(p, C);
+  const float2 *sens = p.sens.as<float2>();
+  const bool combine = stage == GNUFFT_DEAPODIZATION && sens;
+  const bool conv = stage == GNUFFT_CONVOLUTION ||
+                    stage == GNUFFT_DENSITY_ESTIMATION;
+  const size_t per_out = conv ? (size_t)p.g.grid_count
+                              : (size_t)p.g.img_count;
+  for (uint32_t c0 = 0; c0 < C; c0 += step)
+  {
+    const uint32_t n = std::min(step, C - c0);
+    adjoint_batched(p, k + (size_t)c0 * p.M,
+                    combine ? img : img + (size_t)c0 * per_out, n, stage, s,
+                    sens ? sens + (size_t)c0 * p.g.img_count : nullptr,
+                    combine && c0 > 0);
+  }
+}
+
+void forward_chunked(gnufft_plan &p, const float2 *img, float2 *k,
+                     uint32_t C, int stage, cudaStream_t s)
+{
+  const uint32_t step = coils_per_pass(p, C);
+  const float2 *sens = p.sens.as<float2>();
+  const size_t N = (size_t)p.g.img_count;
+  for (uint32_t c0 = 0; c0 < C; c0 += step)
+  {
+    const uint32_t n = std::min(step, C - c0);
+    forward_batched(p, sens ? img : img + (size_t)c0 * N,
+                    k + (size_t)c0 * p.M, n, stage, s,
+                    sens ? sens + (size_t)c0 * N : nullptr);
+  }
+}
+
 size_t adjoint_out_count(const gnufft_plan &p, uint32_t C, int stage)
 {
   if (stage == GNUFFT_CONVOLUTION || stage == GNUFFT_DENSITY_ESTIMATION)
@@ -1108,6 +1202,23 @@ gnufft_status gnufft_set_sens_device(gnufft_plan *p, const void *sens,
   });
 }
 
+gnufft_status gnufft_set_memory_limit(gnufft_plan *p, uint64_t bytes)
+{
+  if (!p)
+    return (gnufft_status)fail(kInvalidArgument, "plan is NULL");
+  p->mem_limit = (size_t)bytes;
+  return GNUFFT_SUCCESS;
+}
+
+gnufft_status gnufft_call_scratch_bytes(const gnufft_plan *p,
+                                        uint32_t n_coils, uint64_t *bytes)
+{
+  if (!p || !bytes || !n_coils)
+    return (gnufft_status)fail(kInvalidArgument, "invalid argument");
+  *bytes = (uint64_t)call_scratch_bytes(*p, n_coils);
+  return GNUFFT_SUCCESS;
+}
+
 gnufft_status gnufft_set_copy_wait(gnufft_plan *p, int64_t polls)
 {
   if (!p)
@@ -1162,8 +1273,8 @@ gnufft_status gnufft_adjoint_device(gnufft_plan *p, const void *kspace,
       adjoint_plain(*p, (const float2 *)kspace, (float2 *)image, n_coils,
                     output, s, false);
     else
-      adjoint_batched(*p, (const float2 *)kspace, (float2 *)image, n_coils,
-                      output, s, p->sens.as<float2>());
+      adjoint_chunked(*p, (const float2 *)kspace, (float2 *)image, n_coils,
+                      output, s);
     collect_times(*p, s);
   });
 }
@@ -1204,8 +1315,8 @@ gnufft_status gnufft_forward_device(gnufft_plan *p, const void *image,
       }
     }
     else
-      forward_batched(*p, (const float2 *)image, (float2 *)kspace, n_coils,
-                      output, s, p->sens.as<float2>());
+      forward_chunked(*p, (const float2 *)image, (float2 *)kspace, n_coils,
+                      output, s);
     collect_times(*p, s);
   });
 }
@@ -1236,8 +1347,8 @@ gnufft_status gnufft_adjoint_host(gnufft_plan *p, const void *kspace,
     p->stage_out.ensure(nout * sizeof(float2));
     GN_CUDA(cudaMemcpyAsync(p->stage_in.get(), kspace, nin * sizeof(float2),
                             cudaMemcpyHostToDevice, s));
-    adjoint_batched(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
-                    n_coils, output, s, p->sens.as<float2>());
+    adjoint_chunked(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
+                    n_coils, output, s);
     GN_CUDA(cudaMemcpyAsync(image, p->stage_out.get(), nout * sizeof(float2),
                             cudaMemcpyDeviceToHost, s));
     GN_CUDA(cudaStreamSynchronize(s));
@@ -1275,8 +1386,8 @@ gnufft_status gnufft_forward_host(gnufft_plan *p, const void *image,
         throw Error(st, g_last_error);
     }
     else
-      forward_batched(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
-                      n_coils, output, s, p->sens.as<float2>());
+      forward_chunked(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
+                      n_coils, output, s);
     GN_CUDA(cudaMemcpyAsync(kspace, p->stage_out.get(), nout * sizeof(float2),
                             cudaMemcpyDeviceToHost, s));
     GN_CUDA(cudaStreamSynchronize(s));

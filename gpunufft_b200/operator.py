@@ -224,6 +224,18 @@ class Plan:
         C.check(C.lib().gnufft_set_sens(self._h, s.ctypes.data, n))
         self.n_sens = n
 
+    def set_memory_limit(self, nbytes: int) -> None:
+        """Cap a call's device scratch (0: the free device memory); calls
+        whose all-coil scratch exceeds it run in coil passes."""
+        C.check(C.lib().gnufft_set_memory_limit(self._h, int(nbytes)))
+
+    def call_scratch_bytes(self, n_coils: int) -> int:
+        """Device scratch the plan holds after a call with n_coils coils."""
+        v = ctypes.c_uint64()
+        C.check(C.lib().gnufft_call_scratch_bytes(self._h, int(n_coils),
+                                                  ctypes.byref(v)))
+        return int(v.value)
+
     def set_timing(self, enable: bool = True) -> None:
         C.check(C.lib().gnufft_set_timing(self._h, int(enable)))
 

@@ -66,35 +66,62 @@ def _key(req: Request) -> str:
     return h.hexdigest()
 
 
-def estimate_bytes(req: Request) -> int:
-    """Device bytes a request needs while it runs: the operator's tables
-    and scratch plus the CG vectors."""
+def plan_table_bytes(req: Request) -> int:
+    """Upper bound of the device bytes of a new operator for the request's
+    trajectory before any call: sorted trajectory, indices (sorted order,
+    sector, inverse), density weights, the interpolation matrix (row offsets
+    per grid cell, at most (kw + 1)^d entries of 8 bytes per sample), the
+    forward work items and column ranges, deapodization, the lookup table
+    and the maps the request sets."""
     dims = [v for v in req.img_dims if v]
     dim = len(dims)
     M = req.traj.shape[1]
-    Cn = req.kspace.shape[0]
     N = int(np.prod(dims))
-    G = int(np.prod([int(np.ceil(v * req.osf)) for v in dims]))
-    lanes = Cn if Cn <= 16 else (Cn + 31) // 32 * 32
-    kw = req.kernel_width
-    nnz = M * kw ** dim
-    tables = M * (4 * dim + 16) + 8 * nnz + 4 * G + 4 * N
-    scratch = 8 * M * lanes + 2 * 8 * Cn * G          # sorted k-space, grid,
-    scratch += 8 * Cn * G                              # cuFFT work area
-    vectors = 8 * Cn * M * 2 + 8 * Cn * N + 8 * N * 6  # data, maps, CG
-    vectors += 8 * Cn * M + 8 * N * 4    # the iteration graph's own buffers
-    return int(tables + scratch + vectors)
+    grid = [int(v * req.osf) for v in dims]
+    G = int(np.prod(grid))
+    Cn = req.kspace.shape[0]
+    nnz = M * (req.kernel_width + 1) ** dim
+    b = 4 * dim * M + 3 * 4 * M + 4 * M + 4 * (G + 1) + 8 * nnz
+    b += 16 * (M // 256 + int(np.prod([-(-g // req.sector_width)
+                                       for g in grid])) + 1)
+    b += 8 * grid[0] * grid[1] + 4 * N + 4 * 4096 + 8 * Cn * N
+    return int(b)
+
+
+def request_bytes(req: Request, plan: Optional[Plan] = None) -> int:
+    """Device bytes a request holds while it runs: its operator (the cached
+    instance's own figure, else plan_table_bytes), the operator's scratch
+    for the request's coil count (gnufft_call_scratch_bytes), and its
+    tensors -- k-space and maps, the CG vectors x, r, p and the
+    temporaries of one iteration (forward output, adjoint outputs)."""
+    dims = [v for v in req.img_dims if v]
+    M = req.traj.shape[1]
+    N = int(np.prod(dims))
+    Cn = req.kspace.shape[0]
+    if plan is not None:
+        op = plan.info.device_bytes + plan.call_scratch_bytes(Cn)
+    else:
+        G = int(np.prod([int(v * req.osf) for v in dims]))
+        lanes = Cn if Cn <= 16 else (Cn + 31) // 32 * 32
+        # scratch bound: sorted k-space lanes, grid and two transform
+        # buffers of a grid each (what gnufft_call_scratch_bytes counts,
+        # rounded up)
+        op = plan_table_bytes(req) + 8 * M * lanes + 3 * 8 * (Cn + 1) * G
+    tensors = 8 * Cn * M + 8 * Cn * N          # k-space, maps
+    tensors += 8 * N * 3                       # x, r, p
+    tensors += 8 * Cn * M + 8 * N * 4          # one iteration's temporaries
+    return int(op + tensors)
 
 
 class PlanCache:
     """Operators resident per trajectory (sector tables, interpolation
     matrix, transform plans and scratch).  At most ``max_instances``
-    instances of one trajectory's operator exist; a request whose
-    trajectory's instances are all busy waits for one (building another
-    costs more than most requests' whole solve).  Idle instances stay cached
-    until memory is needed."""
+    instances of one trajectory's operator exist (two: a second request of
+    the same trajectory runs beside the first); a request whose
+    trajectory's instances are all busy waits for one.  Idle instances stay
+    cached until memory is needed."""
 
-    def __init__(self, device: int = 0, max_instances: int = 1):
+    def __init__(self, device: int = 0, max_instances: int = 2):
         self.device = device
         self.max_instances = max_instances
         self.free: Dict[str, List[Plan]] = collections.defaultdict(list)
@@ -108,6 +135,11 @@ class PlanCache:
     def available(self, req: Request) -> bool:
         key = _key(req)
         return bool(self.free[key]) or self.count[key] < self.max_instances
+
+    def peek(self, req: Request) -> Optional[Plan]:
+        """An idle cached instance for the request's trajectory, if any."""
+        ps = self.free.get(_key(req))
+        return ps[-1] if ps else None
 
     def acquire(self, req: Request) -> Plan:
         key = _key(req)
@@ -161,9 +193,10 @@ class _Active:
     iteration no longer grows with the number of kernels in it."""
 
     def __init__(self, req: Request, plan: Plan, device: int,
-                 use_graph: bool = True):
+                 use_graph: bool = True, admitted_bytes: int = 0):
         self.req = req
         self.plan = plan
+        self.admitted_bytes = admitted_bytes
         self.stream = torch.cuda.Stream(device=device)
         self.done_event = torch.cuda.Event()
         self.it = 0
@@ -252,14 +285,17 @@ class Server:
         self.peak_in_use = 0
         self.peak_device_used = 0
         self.max_concurrent = 0
+        self.peak_live = 0
+        self.peak_accounted = 0
         self._t0 = time.perf_counter()
         self._free0 = free
+        self._torch0 = torch.cuda.memory_allocated(device)
 
     def now(self) -> float:
         return time.perf_counter() - self._t0
 
     def submit(self, req: Request) -> None:
-        if estimate_bytes(req) > self.budget:
+        if request_bytes(req) > self.budget:
             raise ValueError("request larger than the server's memory budget")
         if req.arrival <= 0:
             req.arrival = self.now()
@@ -275,18 +311,29 @@ class Server:
             if not self.cache.available(req):
                 waiting.append(req)
                 continue
-            need = estimate_bytes(req)
-            while (self.in_use + need + self.cache.idle_bytes() > self.budget
+            cached = self.cache.peek(req)
+            need = request_bytes(req, cached)
+            idle = self.cache.idle_bytes()
+            if cached is not None:  # counted in `need` from now on
+                idle -= cached.info.device_bytes
+            while (self.in_use + need + idle > self.budget
                    and self.cache.evict_one()):
-                pass
+                idle = self.cache.idle_bytes()
+                cached = self.cache.peek(req)
+                need = request_bytes(req, cached)
+                if cached is not None:
+                    idle -= cached.info.device_bytes
             if self.in_use + need > self.budget:
                 waiting.append(req)         # wait for memory to free up
                 break
             req.admitted = self.now()
             plan = self.cache.acquire(req)
-            self.active.append(_Active(req, plan, self.device))
+            self.active.append(_Active(req, plan, self.device,
+                                       admitted_bytes=need))
             self.in_use += need
             self.peak_in_use = max(self.peak_in_use, self.in_use)
+            self.peak_accounted = max(self.peak_accounted,
+                                      self.in_use + self.cache.idle_bytes())
         waiting.extend(self.queue)
         self.queue = waiting
         self.max_concurrent = max(self.max_concurrent, len(self.active))
@@ -299,7 +346,7 @@ class Server:
                 a.req.finished = self.now()
                 a.release()
                 self.cache.release(a.plan)
-                self.in_use -= estimate_bytes(a.req)
+                self.in_use -= a.admitted_bytes
                 self.done.append(a.req)
             else:
                 keep.append(a)
@@ -314,6 +361,16 @@ class Server:
                 a.step()
         free, total = torch.cuda.mem_get_info(self.device)
         self.peak_device_used = max(self.peak_device_used, total - free)
+        # what the running requests and cached operators hold: operators'
+        # own figures and the tensors torch has allocated (not the memory
+        # its caching allocator keeps for reuse)
+        live = (sum(a.plan.info.device_bytes for a in self.active) +
+                self.cache.idle_bytes() +
+                max(0, torch.cuda.memory_allocated(self.device) -
+                    self._torch0))
+        self.peak_live = max(self.peak_live, live)
+        self.peak_accounted = max(self.peak_accounted,
+                                  self.in_use + self.cache.idle_bytes())
 
     def run(self, arrivals: Sequence[Request], timeout: float = 600.0):
         """Replay ``arrivals`` (sorted by ``arrival`` seconds from now) and
@@ -349,7 +406,8 @@ class Server:
             "throughput_rps": len(self.done) / span if span > 0 else None,
             "max_concurrent": self.max_concurrent,
             "peak_hbm_gb": self.peak_device_used / 1e9,
-            "peak_admitted_estimate_gb": self.peak_in_use / 1e9,
+            "peak_live_gb": self.peak_live / 1e9,
+            "peak_admitted_gb": self.peak_accounted / 1e9,
             "plan_cache_hits": self.cache.hits,
             "plan_cache_misses": self.cache.misses,
         }

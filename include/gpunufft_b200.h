@@ -269,6 +269,22 @@ typedef struct gnufft_stage_times {
 } gnufft_stage_times;
 GNUFFT_API gnufft_status gnufft_set_timing(gnufft_plan *plan, int enable);
 
+/* Device memory of a call.  The plan's scratch buffers (sorted k-space,
+ * grid, transform buffers) grow on first use to what a call with n_coils
+ * coils needs (gnufft_call_scratch_bytes reports that figure) and are kept.
+ * A call whose scratch for all its coils would not fit the plan's memory
+ * limit -- by default the device memory free at the call plus the scratch
+ * the plan holds already, less 256 MiB -- runs in passes of as many coils
+ * as fit (at least one), like the upstream's concurrent coil count
+ * (gpuNUFFT_operator.cpp:327-368, there for 2-D only); results are the
+ * same up to the order of the coil sum.  gnufft_set_memory_limit sets the
+ * limit in bytes (0: the free memory). */
+GNUFFT_API gnufft_status gnufft_set_memory_limit(gnufft_plan *plan,
+                                                 uint64_t bytes);
+GNUFFT_API gnufft_status gnufft_call_scratch_bytes(const gnufft_plan *plan,
+                                                   uint32_t n_coils,
+                                                   uint64_t *bytes);
+
 /* Tile copies of this library's kernels complete on a bounded wait: a copy
  * that has not completed after the wait's polls sets a flag, the block
  * stops (after a bounded wait for its copies in flight) and the call

@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from oracle import nufft_oracle as O
-from tests.helpers import cplx, rel_l2
+from tests.helpers import cplx, gaussian_maps, kooshball_3d, radial_2d, rel_l2
 
 pytestmark = pytest.mark.gpu
 
@@ -86,3 +86,37 @@ def test_sixteen_coil_group(dims, n_coils):
     rng = np.random.default_rng(8)
     traj = rng.uniform(-0.5, 0.5, (len(dims), 3000)).astype(np.float32)
     _check(traj, dims, n_coils, 9)
+
+
+@pytest.mark.parametrize("dims", [(16, 16, 16), (48, 40)])
+def test_coil_passes_under_a_memory_limit(dims):
+    """A plan whose memory limit admits only a few coils' scratch runs a
+    call in coil passes (the upstream's concurrent coil count,
+    gpuNUFFT_operator.cpp:327-368): the same results as one pass, for the
+    coil-combined adjoint, the per-coil stages and the forward; a limit
+    below one coil's scratch still runs, one coil per pass."""
+    import gpunufft_b200 as G
+    from oracle import nufft_oracle as O
+    rng = np.random.default_rng(31)
+    C = 12
+    traj = (kooshball_3d(200, 32) if len(dims) == 3 else
+            radial_2d(48, 96)).astype(np.float32)
+    g = O.make_geometry(dims, 2.0, 3, 8)
+    maps = gaussian_maps(C, g.img_shape, rng)
+    k = cplx(rng, C, traj.shape[1])
+    x = cplx(rng, *g.img_shape)
+    one = G.Plan(traj, dims, 3, 8, 2.0, None, maps, G.BALANCED)
+    split = G.Plan(traj, dims, 3, 8, 2.0, None, maps, G.BALANCED)
+    try:
+        assert split.call_scratch_bytes(5) < split.call_scratch_bytes(C)
+        exp_adj = one.adjoint(k)
+        exp_fwd = one.forward(x)
+        exp_fft = one.adjoint(k, G.FFT)
+        for limit in (split.call_scratch_bytes(5), 1):
+            split.set_memory_limit(limit)
+            assert rel_l2(split.adjoint(k), exp_adj) < 1e-6
+            assert rel_l2(split.forward(x), exp_fwd) < 1e-6
+            assert rel_l2(split.adjoint(k, G.FFT), exp_fft) < 1e-6
+    finally:
+        one.close()
+        split.close()

@@ -60,6 +60,9 @@ def test_results_alone_and_in_the_mix():
     for r in done:
         assert rel_l2(r.result, alone[r.rid]) < TOL, r.rid
     assert st["p99_ms"] >= st["p50_ms"] > 0
+    # the admission accounting covers what requests and cached operators
+    # actually held (operators' own figures plus allocated tensors)
+    assert st["peak_admitted_gb"] >= st["peak_live_gb"] > 0
 
 
 def test_results_match_the_direct_solver():
@@ -77,9 +80,9 @@ def test_results_match_the_direct_solver():
 
 
 def test_memory_based_admission():
-    from gpunufft_b200.serving import Server, estimate_bytes
+    from gpunufft_b200.serving import Server, request_bytes
     reqs = _requests()[:3]
-    need = sorted(estimate_bytes(r) for r in reqs)
+    need = sorted(request_bytes(r) for r in reqs)
     # room for the two smallest at once, never for all three
     budget = need[0] + need[1] + need[0] // 2
     s = Server(max_slots=8, memory_budget=max(budget, need[2]))
@@ -90,9 +93,9 @@ def test_memory_based_admission():
         s.close()
     assert len(done) == 3
     assert st["max_concurrent"] <= 2
-    assert st["peak_admitted_estimate_gb"] * 1e9 <= max(budget, need[2])
+    assert st["peak_admitted_gb"] * 1e9 <= max(budget, need[2])
     big = _requests()[3]
-    s2 = Server(memory_budget=estimate_bytes(big) - 1)
+    s2 = Server(memory_budget=request_bytes(big) - 1)
     with pytest.raises(ValueError):
         s2.submit(big)
     s2.close()
