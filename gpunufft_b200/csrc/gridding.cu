@@ -1145,16 +1145,22 @@ __global__ void __launch_bounds__(kThreads)
 
 // The same interpolation with every coil group of an item in one block (3-D
 // grids written with coil pairs interleaved, cell q of coil c at
-// ((c / 2) * G + q) * 2 + c % 2): each thread computes the footprints of
-// its (at most two) samples once, in registers, and the block walks the
-// coil groups through a ring of `nbuf` tile buffers; the copy of group
-// g + nbuf is issued as soon as group g's buffer is released, so nbuf - 1
-// copies overlap each group's accumulation.  A tile is one 5-D box {2 coils,
-// pad, pad, pad, CG / 2 pairs}: its innermost extent is a coil pair (16
-// bytes), so the sector's x start needs no rounding, and one 16-byte shared
-// load reads two coils of a cell.  Per sample and coil the arithmetic
-// (cell order z, y, x; weight (wz * wy) * wx; one fused multiply-add per
-// cell) is that of k_forward_tma.
+// ((c / 2) * G + q) * 2 + c % 2).  Each thread computes the footprint of
+// its (at most two) samples once, in registers; the samples of an item are
+// taken in the plan's lane order (build_forward_lane_order), which puts
+// samples whose footprints start in different shared-memory bank groups on
+// each eight adjacent lanes, so that the 16-byte tile reads of a quarter
+// warp, which all lanes make at the same footprint offset, do not collide.
+// The block walks the coil groups through a ring of `nbuf` tile buffers; the copy of group g + nbuf is issued as soon
+// as group g's buffer is released, so nbuf - 1 copies overlap each group's
+// accumulation.  A tile is one 4-D box {2 pad, pad, pad, CG / 2 pairs}
+// whose innermost axis runs over x with the two coils of a pair interleaved
+// (2 G_x values of 8 bytes): a box row is a tile row of both coils (160
+// bytes at pad 10) rather than a single cell, the sector's x start (2 x 8
+// bytes per cell) needs no rounding, and one 16-byte shared load reads two
+// coils of a cell.  Per sample and coil the arithmetic (cell order z, y, x;
+// weight (wz * wy) * wx; one fused multiply-add per cell) is that of
+// k_forward_tma.
 // Shared memory: nbuf tiles [CG / 2][pad][pad][pad][2] | nbuf mbarriers |
 // flag.
 constexpr int kFwdSpt = (kFwdItemSamples + kThreads - 1) / kThreads;
@@ -1169,6 +1175,7 @@ template <int CG, int KS, int MINB>
 __global__ void __launch_bounds__(kThreads, MINB)
     k_forward_tma_groups(const __grid_constant__ CUtensorMap tmap,
                          const FwdItem *__restrict__ items,
+                         const uint32_t *__restrict__ order,
                          const float *__restrict__ traj,
                          const uint32_t *__restrict__ idx,
                          const float *__restrict__ dens,
@@ -1212,11 +1219,10 @@ __global__ void __launch_bounds__(kThreads, MINB)
         "r"(tbytes)
         : "memory");
     asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::"
-        "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(
-            dst),
-        "l"(tm), "r"(0), "r"(base[0]), "r"(base[1]), "r"(base[2]),
-        "r"(gi * NP), "r"(bar)
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::"
+        "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+        "l"(tm), "r"(2 * base[0]), "r"(base[1]), "r"(base[2]), "r"(gi * NP),
+        "r"(bar)
         : "memory");
   };
   if (inside && threadIdx.x == 0)
@@ -1232,25 +1238,39 @@ __global__ void __launch_bounds__(kThreads, MINB)
   }
 
   // footprints of this thread's samples (tile frame), kept for all groups
+  // footprint, original position and sqrt(density) of this thread's
+  // samples (the item's samples in lane order), kept for all coil groups
   int l0[kFwdSpt][3], n[kFwdSpt][3];
   float w[kFwdSpt][3][KS];
+  uint32_t jdst[kFwdSpt];
+  float sdv[kFwdSpt];
 #pragma unroll
   for (int s = 0; s < kFwdSpt; ++s)
   {
-    const int t = it.begin + threadIdx.x + s * kThreads;
+    const int k = it.begin + threadIdx.x + s * kThreads;
+    const bool live = k < it.end;
+    const uint32_t t = live ? (order ? __ldg(order + k) : (uint32_t)k) : 0u;
+    jdst[s] = 0;
+    sdv[s] = 1.0f;
+    if (live)
+    {
+      jdst[s] = __ldg(idx + t);
+      if (dens)
+        sdv[s] = sqrtf(__ldg(dens + t));
+    }
 #pragma unroll
     for (int a = 0; a < 3; ++a)
     {
       int l[KS];
       n[s][a] = 0;
-      if (t < it.end)
+      if (live)
         n[s][a] = compact_axis<KS>(__ldg(traj + (size_t)a * M + t), a, sa[a],
                                    g, lut, l, w[s][a]);
       else
       {
 #pragma unroll
-        for (int k = 0; k < KS; ++k)
-          w[s][a][k] = 0.f;
+        for (int k2 = 0; k2 < KS; ++k2)
+          w[s][a][k2] = 0.f;
         l[0] = 0;
       }
       l0[s][a] = l[0];
@@ -1314,11 +1334,25 @@ __global__ void __launch_bounds__(kThreads, MINB)
       __syncthreads();
     }
 
+    // performFFTScaling then performDensityCompensation
+    // (std_gpuNUFFT_kernels.cu:114-140, 220-242)
+    auto emit = [&](int c, float2 a, int s) {
+      const int cc = gi * CG + c;
+      if (cc < C)
+      {
+        float ax = __fmul_rn(a.x, scale), ay = __fmul_rn(a.y, scale);
+        if (dens)
+        {
+          ax = __fmul_rn(ax, sdv[s]);
+          ay = __fmul_rn(ay, sdv[s]);
+        }
+        out[(size_t)cc * M + jdst[s]] = make_float2(ax, ay);
+      }
+    };
 #pragma unroll
     for (int s = 0; s < kFwdSpt; ++s)
     {
-      const int t = it.begin + threadIdx.x + s * kThreads;
-      if (t >= it.end)
+      if (it.begin + threadIdx.x + s * kThreads >= it.end)
         continue;
       float2 acc[CG];
 #pragma unroll
@@ -1359,26 +1393,9 @@ __global__ void __launch_bounds__(kThreads, MINB)
           }
         }
       }
-      const uint32_t j = __ldg(idx + t);
-      const float sd = dens ? sqrtf(__ldg(dens + t)) : 1.0f;
 #pragma unroll
       for (int c = 0; c < CG; ++c)
-      {
-        const int cc = gi * CG + c;
-        if (cc < C)
-        {
-          // performFFTScaling then performDensityCompensation
-          // (std_gpuNUFFT_kernels.cu:114-140, 220-242)
-          float ax = __fmul_rn(acc[c].x, scale),
-                ay = __fmul_rn(acc[c].y, scale);
-          if (dens)
-          {
-            ax = __fmul_rn(ax, sd);
-            ay = __fmul_rn(ay, sd);
-          }
-          out[(size_t)cc * M + j] = make_float2(ax, ay);
-        }
-      }
+        emit(c, acc[c], s);
     }
     __syncthreads();  // this group's buffer is free
     if (inside && threadIdx.x == 0 && gi + nbuf < ng)
@@ -1824,13 +1841,82 @@ bool forward_pairs(const Geo &g, int tile_coils)
   return 2 * tile + 64 <= 74 * 1024;
 }
 
+// One block per work item: the bank group (16-byte unit mod 8) of each
+// sample's first footprint cell in the coil-pair tile, then the samples
+// dealt round-robin over the eight groups: position = the samples of lower
+// rank within their group, plus those of equal rank in lower groups.  Each
+// run of eight lanes then holds eight groups while all of them have
+// samples left.  Only the lanes' order changes: every sample's arithmetic
+// is the same in any position.
+template <int KS>
+__global__ void __launch_bounds__(kThreads)
+    k_forward_lane_order(const FwdItem *__restrict__ items,
+                         const float *__restrict__ traj, uint32_t M, Geo g,
+                         const float *__restrict__ lut,
+                         uint32_t *__restrict__ order)
+{
+  __shared__ unsigned char s_bank[kFwdItemSamples];
+  __shared__ int s_cnt[8];
+  const FwdItem it = items[blockIdx.x];
+  const int n = it.end - it.begin;
+  int sa[3];
+  split_sector(it.sector, g, sa);
+  if (threadIdx.x < 8)
+    s_cnt[threadIdx.x] = 0;
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += kThreads)
+  {
+    int l0[3];
+    for (int a = 0; a < 3; ++a)
+    {
+      int l[KS];
+      float w[KS];
+      const int nn = compact_axis<KS>(
+          __ldg(traj + (size_t)a * M + it.begin + k), a, sa[a], g, lut, l, w);
+      l0[a] = nn ? l[0] : 0;
+    }
+    const int bank = ((l0[2] * g.pad + l0[1]) * g.pad + l0[0]) & 7;
+    s_bank[k] = (unsigned char)bank;
+    atomicAdd(&s_cnt[bank], 1);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < n; k += kThreads)
+  {
+    const int b = s_bank[k];
+    int rank = 0;
+    for (int u = 0; u < k; ++u)
+      rank += s_bank[u] == b;
+    int pos = 0;
+    for (int q = 0; q < 8; ++q)
+      pos += min(s_cnt[q], rank) + (q < b && s_cnt[q] > rank);
+    order[it.begin + pos] = (uint32_t)(it.begin + k);
+  }
+}
+
+void build_forward_lane_order(const FwdItem *items, int n_items,
+                              const float *traj_sorted, uint32_t M,
+                              const Geo &g, const float *lut, uint32_t *order,
+                              cudaStream_t s)
+{
+  if (n_items <= 0)
+    return;
+  if (slots_for(g) == 4)
+    k_forward_lane_order<4><<<(unsigned)n_items, kThreads, 0, s>>>(
+        items, traj_sorted, M, g, lut, order);
+  else
+    k_forward_lane_order<8><<<(unsigned)n_items, kThreads, 0, s>>>(
+        items, traj_sorted, M, g, lut, order);
+  GN_LAUNCH_CHECK("forward lane order");
+}
+
 bool launch_forward_interp_tma(const FwdItem *items, int n_items,
                                const float *traj_sorted, const uint32_t *idx,
                                const float *dens_sorted, const float2 *grid,
                                const Geo &g, const float *lut, uint32_t M,
                                int C, float scale, float2 *out,
                                tma::CopyWait cw, cudaStream_t s,
-                               int tile_coils, bool paired)
+                               int tile_coils, bool paired,
+                               const uint32_t *lane_order)
 {
   if (n_items <= 0)
     return true;
@@ -1843,17 +1929,18 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
     const int pad = g.pad;
     const int pairs = (C + 1) / 2;
     CUtensorMap tm;
-    cuuint64_t dims[5] = {2, (cuuint64_t)g.G[0], (cuuint64_t)g.G[1],
+    // the coil of a pair and x merged into one axis of 2 G_x values: a box
+    // row is a tile row of both coils (2 pad x 8 bytes), not one cell
+    cuuint64_t dims[4] = {2 * (cuuint64_t)g.G[0], (cuuint64_t)g.G[1],
                           (cuuint64_t)g.G[2], (cuuint64_t)pairs};
-    cuuint64_t strides[4];
-    strides[0] = 2 * sizeof(float2);
-    strides[1] = strides[0] * g.G[0];
-    strides[2] = strides[1] * g.G[1];
-    strides[3] = strides[2] * g.G[2];
-    cuuint32_t box[5] = {2, (cuuint32_t)pad, (cuuint32_t)pad,
+    cuuint64_t strides[3];
+    strides[0] = 2 * sizeof(float2) * (cuuint64_t)g.G[0];
+    strides[1] = strides[0] * g.G[1];
+    strides[2] = strides[1] * g.G[2];
+    cuuint32_t box[4] = {2 * (cuuint32_t)pad, (cuuint32_t)pad,
                          (cuuint32_t)pad, 2};
-    cuuint32_t estr[5] = {1, 1, 1, 1, 1};
-    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 5, const_cast<float2 *>(grid),
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, const_cast<float2 *>(grid),
             dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
@@ -1864,9 +1951,9 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
     auto k = k_forward_tma_groups<4, 4, 3>;
     GN_CUDA(cudaFuncSetAttribute(
         k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2));
-    k<<<(unsigned)n_items, kThreads, smem2, s>>>(tm, items, traj_sorted, idx,
-                                                dens_sorted, grid, g, lut, M,
-                                                C, nbuf, scale, out, cw);
+    k<<<(unsigned)n_items, kThreads, smem2, s>>>(
+        tm, items, lane_order, traj_sorted, idx, dens_sorted, grid, g, lut, M,
+        C, nbuf, scale, out, cw);
     GN_LAUNCH_CHECK("forward interpolation (coil-pair tiles, all groups)");
     return true;
   }

@@ -107,7 +107,17 @@ bool launch_forward_interp_tma(const FwdItem *items, int n_items,
                                const Geo &g, const float *lut, uint32_t M,
                                int C, float scale, float2 *out,
                                tma::CopyWait cw, cudaStream_t s,
-                               int tile_coils = 0, bool paired = false);
+                               int tile_coils = 0, bool paired = false,
+                               const uint32_t *lane_order = nullptr);
+
+// The order in which the coil-pair forward (3-D) takes each work item's
+// samples: `order` [M] lists, per item, sorted sample indices such that
+// each eight adjacent lanes read their tile cells from different
+// shared-memory bank groups.  Performance only: results do not depend on it.
+void build_forward_lane_order(const FwdItem *items, int n_items,
+                              const float *traj_sorted, uint32_t M,
+                              const Geo &g, const float *lut, uint32_t *order,
+                              cudaStream_t s);
 
 // Whether the 3-D forward of this geometry runs on a grid written with coil
 // pairs interleaved (cell q of coil c at ((c / 2) * G + q) * 2 + c % 2;

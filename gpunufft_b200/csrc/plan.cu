@@ -92,7 +92,7 @@ struct gnufft_plan
 
   // resident device tables
   DeviceBuffer lut, traj_sorted, di, sec_sorted, dens_sorted;
-  DeviceBuffer fwd_items, deapo, sens;
+  DeviceBuffer fwd_items, fwd_order, deapo, sens;
   DeviceBuffer di_inv;  // sorted position of every original sample
   DeviceBuffer w_rows, w_nz;  // interpolation matrix, CSR by grid cell
   DeviceBuffer dlut;          // kernel derivative table (trajectory gradient)
@@ -142,7 +142,8 @@ struct gnufft_plan
   {
     const DeviceBuffer *bufs[] = {&lut,         &traj_sorted, &di,
                                   &sec_sorted,  &dens_sorted,
-                                  &fwd_items,   &deapo,       &sens,
+                                  &fwd_items,   &fwd_order,   &deapo,
+                                  &sens,
                                   &di_inv,
                                   &w_rows,      &w_nz,
                                   &ks,          &grid,        &stage_in,
@@ -423,6 +424,14 @@ void finish_tables(gnufft_plan &p)
                               p.sec_sorted.as<uint32_t>(), p.M, p.g,
                               p.lut.as<float>(), p.w_rows, p.w_nz, p.stream);
   build_items(p);
+  if (p.dim == 3 && forward_pairs(p.g, 0))
+  {
+    p.fwd_order.reset((size_t)p.M * sizeof(uint32_t));
+    build_forward_lane_order(p.fwd_items.as<FwdItem>(), p.n_fwd_items,
+                             p.traj_sorted.as<float>(), p.M, p.g,
+                             p.lut.as<float>(), p.fwd_order.as<uint32_t>(),
+                             p.stream);
+  }
   p.di_inv.reset((size_t)p.M * sizeof(uint32_t) + 4);
   launch_invert_permutation(p.di.as<uint32_t>(), p.M, p.di_inv.as<uint32_t>(),
                             p.stream);
@@ -767,7 +776,7 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
             p.traj_sorted.as<float>(), p.di.as<uint32_t>(),
             p.has_dens ? p.dens_sorted.as<float>() : nullptr, grid, g,
             p.lut.as<float>(), p.M, (int)C, g.fft_scale, k, copy_wait(p), s,
-            p.fwd_tile_coils, paired))
+            p.fwd_tile_coils, paired, p.fwd_order.as<uint32_t>()))
       launch_forward_interp(
           p.fwd_items.as<FwdItem>(), p.n_fwd_items, p.traj_sorted.as<float>(),
           p.di.as<uint32_t>(),
