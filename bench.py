@@ -753,9 +753,12 @@ def serving_run(dev, n_requests, seed=0):
 def batch_run(dev, steps, warmup, seed=0, n_instances=64):
     """``n_instances`` uneven 2-D spiral operators (image 96-320^2, 8-32
     coils, 10k-120k samples, osf 1.25-2, kernel width 3-5; sector width and
-    forward tile from the autotuner): fwd + adj of every instance per step,
-    replayed from one CUDA graph, against the plain per-instance loop.
-    Device-timed ms per step of both."""
+    forward tile from the autotuner): fwd + adj of every instance per step.
+    Headline: the persistent batch (every stage of all instances in one
+    launch, one cuFFT call per instance between stages) replayed from a
+    CUDA graph; beside it the instances' own launches captured on 8
+    streams into one graph, and the plain per-instance loop on one stream.
+    Device-timed ms per step of each."""
     import torch
 
     import gpunufft_b200 as G
@@ -789,7 +792,8 @@ def batch_run(dev, steps, warmup, seed=0, n_instances=64):
                             device=dev, tile_coils=tr.tile_coils))
         coils.append(s["n_coils"])
     tune_s = time.perf_counter() - t0
-    bo = BatchedOperator(plans, coils, n_streams=8, device=dev)
+    bo = BatchedOperator(plans, coils, device=dev, mode="persistent")
+    info = bo.info()
     for x in bo.img_in:
         x.copy_(torch.randn_like(x))
     for k in bo.k_in:
@@ -800,6 +804,25 @@ def batch_run(dev, steps, warmup, seed=0, n_instances=64):
     ms_plain, _ = timed_steps(lambda: (bo.plain("forward"),
                                        bo.plain("adjoint")), steps,
                               max(warmup, 1))
+    # one more persistent step inside an NVTX range, untimed, so that a
+    # profiler can list exactly the launches of one step
+    # (ncu --nvtx --nvtx-include "batch_step/")
+    torch.cuda.nvtx.range_push("batch_step")
+    bo.replay("forward")
+    bo.replay("adjoint")
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize(dev)
+    bo.close()
+    so = BatchedOperator(plans, coils, n_streams=8, device=dev,
+                         mode="streams")
+    for x in so.img_in:
+        x.copy_(torch.randn_like(x))
+    for k in so.k_in:
+        k.copy_(torch.randn_like(k))
+    ms_streams, _ = timed_steps(lambda: (so.replay("forward"),
+                                         so.replay("adjoint")), steps,
+                                max(warmup, 1))
+    del so
     sw_hist = {}
     for sw, tc in tuned:
         key = f"sw{sw}/tile{tc or 'auto'}"
@@ -809,9 +832,18 @@ def batch_run(dev, steps, warmup, seed=0, n_instances=64):
     n = len(plans)
     return {"value": n / (ms_graph * 1e-3), "unit": "instances/s",
             "ms_per_step": ms_graph, "instances": n,
+            "launches_per_step": {
+                "persistent_kernels": info.kernels_forward +
+                info.kernels_adjoint,
+                "fft_calls": 2 * info.fft_calls,
+                "units": dict(zip(("prepare", "interpolation", "gather",
+                                   "spread", "finish"), info.units))},
+            "streams_graph": {"value": n / (ms_streams * 1e-3),
+                              "ms_per_step": ms_streams},
             "plain": {"value": n / (ms_plain * 1e-3),
                       "ms_per_step": ms_plain},
             "graph_over_plain": ms_plain / ms_graph,
+            "persistent_over_streams": ms_streams / ms_graph,
             "autotune": {"seconds": tune_s, "choices": sw_hist},
             "workload": f"{n} variable-density 2-D spirals, image 96-320^2, "
                         "8-32 coils, 10k-120k samples, osf 1.25-2, kw 3-5, "

@@ -48,6 +48,8 @@ EXPORTED = (
     "gnufft_traj_grad_device", "gnufft_set_sens_device",
     "gnufft_set_copy_wait", "gnufft_plan_check",
     "gnufft_set_memory_limit", "gnufft_call_scratch_bytes",
+    "gnufft_batch_create", "gnufft_batch_forward", "gnufft_batch_adjoint",
+    "gnufft_batch_get_info", "gnufft_batch_destroy",
 )
 
 
@@ -83,6 +85,15 @@ class StageTimes(ctypes.Structure):
                 ("fft_ms", ctypes.c_float),
                 ("finish_ms", ctypes.c_float),
                 ("launches", ctypes.c_uint32)]
+
+
+class BatchInfo(ctypes.Structure):
+    _fields_ = [("n_instances", ctypes.c_uint32),
+                ("units", ctypes.c_uint32 * 5),
+                ("kernels_forward", ctypes.c_uint32),
+                ("kernels_adjoint", ctypes.c_uint32),
+                ("fft_calls", ctypes.c_uint32),
+                ("device_bytes", ctypes.c_uint64)]
 
 
 class GnufftError(RuntimeError):
@@ -151,6 +162,16 @@ def lib() -> ctypes.CDLL:
     L.gnufft_set_timing.argtypes = [_P, ctypes.c_int]
     L.gnufft_get_stage_times.restype = st
     L.gnufft_get_stage_times.argtypes = [_P, ctypes.POINTER(StageTimes)]
+    L.gnufft_batch_create.restype = st
+    L.gnufft_batch_create.argtypes = [_P, _P, _U, ctypes.POINTER(_P)]
+    for name in ("gnufft_batch_forward", "gnufft_batch_adjoint"):
+        f = getattr(L, name)
+        f.restype = st
+        f.argtypes = [_P, _P, _P, _P]
+    L.gnufft_batch_get_info.restype = st
+    L.gnufft_batch_get_info.argtypes = [_P, ctypes.POINTER(BatchInfo)]
+    L.gnufft_batch_destroy.restype = st
+    L.gnufft_batch_destroy.argtypes = [_P]
     L.gnufft_last_error.restype = ctypes.c_char_p
     L.gnufft_last_error.argtypes = []
     L.gnufft_status_string.restype = ctypes.c_char_p

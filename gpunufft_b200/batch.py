@@ -1,14 +1,19 @@
-"""Many independent operators in one captured CUDA graph, and the
-autotuner that picks each operator's sector width and tile shape.
+"""Many independent operators run together, and the autotuner that picks
+each operator's sector width and tile shape.
 
 ``BatchedOperator`` takes operators of uneven sizes (image size, coils,
-trajectory length, oversampling, kernel width) and records every
-instance's forward (or adjoint) into one CUDA graph: instances are spread
-over several capture streams, so the graph has independent branches that
-the GPU runs concurrently, and one ``replay`` launches all of them with no
-per-kernel host work.  Inputs and outputs are static device tensors owned
-by the batch; ``forward`` / ``adjoint`` copy new data in, replay, and
-return the (static) outputs.
+trajectory length, oversampling, kernel width, sector width; one plan may
+appear several times, as frames sharing a trajectory).  By default
+(``mode="persistent"``) it runs them through the library's batch entry
+points (``gnufft_batch_forward`` / ``gnufft_batch_adjoint``): every stage
+of all instances -- forward: prepare, interpolation; adjoint: gather,
+spread, finish -- is one persistent launch whose blocks take (instance,
+work item) units from a device counter, with one cuFFT call per instance
+between the stages; the call is captured once into a CUDA graph and
+replayed.  ``mode="streams"`` records the instances' own per-operator
+launches on several capture streams into one graph instead.  Inputs and
+outputs are static device tensors owned by the batch; ``forward`` /
+``adjoint`` copy new data in, replay, and return the (static) outputs.
 
 ``autotune`` times fwd + adj for candidate sector widths and forward tile
 shapes (coils staged per sector tile) on the instance itself and returns
@@ -16,6 +21,7 @@ the fastest.  Results are cached per geometry.
 """
 from __future__ import annotations
 
+import ctypes
 import dataclasses
 from typing import Dict, List, Optional, Sequence, Tuple
 
@@ -114,21 +120,27 @@ def autotune(traj, img_dims: Sequence[int], n_coils: int,
 # batched execution in one CUDA graph
 # --------------------------------------------------------------------------
 class BatchedOperator:
-    """Independent operators replayed together from one CUDA graph.
+    """Independent operators run together (see the module docstring).
 
-    plans: one Plan per instance (built with its own maps if any);
-    n_coils: coil count per instance; n_streams: capture branches."""
+    plans: one Plan per instance (built with its own maps if any; a plan
+    may repeat); n_coils: coil count per instance; mode: "persistent" (one
+    launch per stage for all instances) or "streams" (per-instance launches
+    on n_streams capture branches)."""
 
     def __init__(self, plans: Sequence[Plan], n_coils: Sequence[int],
-                 n_streams: int = 8, device: int = 0):
+                 n_streams: int = 8, device: int = 0,
+                 mode: str = "persistent"):
         if len(plans) != len(n_coils):
             raise ValueError("one coil count per plan")
+        if mode not in ("persistent", "streams"):
+            raise ValueError("mode is 'persistent' or 'streams'")
         self.plans = list(plans)
         self.n_coils = [int(c) for c in n_coils]
         self.device = device
+        self.mode = mode
+        self._batch = None
         dev = torch.device("cuda", device)
-        self.img_in = []
-        self.k_in = []
+        self.img_in, self.k_in, self.k_out, self.img_out = [], [], [], []
         for p, c in zip(self.plans, self.n_coils):
             shape = p.img_shape if p.n_sens else (c,) + p.img_shape
             self.img_in.append(torch.zeros(shape, dtype=torch.complex64,
@@ -139,30 +151,90 @@ class BatchedOperator:
                         for _ in range(max(1, n_streams))]
         self._graphs: Dict[str, torch.cuda.CUDAGraph] = {}
         self._outs: Dict[str, list] = {}
-        # grow every plan's scratch and create its FFT plans before capture
-        for p, x, k in zip(self.plans, self.img_in, self.k_in):
-            p.forward(x)
-            p.adjoint(k)
+        if mode == "persistent":
+            n = len(self.plans)
+            handles = (ctypes.c_void_p * n)(*[p._h.value for p in self.plans])
+            coils = (ctypes.c_uint32 * n)(*self.n_coils)
+            h = ctypes.c_void_p()
+            with torch.cuda.device(device):
+                C.check(C.lib().gnufft_batch_create(handles, coils, n,
+                                                    ctypes.byref(h)))
+            self._batch = h
+            for p, c, x in zip(self.plans, self.n_coils, self.img_in):
+                self.k_out.append(torch.empty((c, p.M), dtype=torch.complex64,
+                                              device=dev))
+                self.img_out.append(torch.empty_like(x))
+
+            def ptrs(ts):
+                return (ctypes.c_void_p * n)(*[t.data_ptr() for t in ts])
+            self._p_img_in, self._p_k_out = ptrs(self.img_in), ptrs(self.k_out)
+            self._p_k_in, self._p_img_out = ptrs(self.k_in), ptrs(self.img_out)
+        # grow every plan's scratch, create its FFT plans and load the
+        # kernels before any capture
+        for i in range(len(self.plans)):
+            self._call_one("forward", i)
+            self._call_one("adjoint", i)
+        if self._batch is not None:
+            self._call_batch("forward")
+            self._call_batch("adjoint")
         torch.cuda.synchronize(device)
 
-    def _call(self, kind: str, i: int):
+    def info(self) -> Optional[C.BatchInfo]:
+        """Work units per stage, launches per call and device bytes of the
+        persistent batch (None in "streams" mode)."""
+        if self._batch is None:
+            return None
+        info = C.BatchInfo()
+        C.check(C.lib().gnufft_batch_get_info(self._batch,
+                                              ctypes.byref(info)))
+        return info
+
+    def close(self) -> None:
+        if self._batch is not None:
+            self._graphs.clear()
+            C.lib().gnufft_batch_destroy(self._batch)
+            self._batch = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call_one(self, kind: str, i: int):
         p = self.plans[i]
         return (p.forward(self.img_in[i]) if kind == "forward"
                 else p.adjoint(self.k_in[i]))
 
+    def _call_batch(self, kind: str) -> list:
+        stream = ctypes.c_void_p(
+            torch.cuda.current_stream(self.device).cuda_stream)
+        L = C.lib()
+        if kind == "forward":
+            C.check(L.gnufft_batch_forward(self._batch, self._p_img_in,
+                                           self._p_k_out, stream))
+            return self.k_out
+        C.check(L.gnufft_batch_adjoint(self._batch, self._p_k_in,
+                                       self._p_img_out, stream))
+        return self.img_out
+
     def _capture(self, kind: str) -> None:
         g = torch.cuda.CUDAGraph()
         main = torch.cuda.Stream(device=self.device)
-        outs = [None] * len(self.plans)
         main.wait_stream(torch.cuda.current_stream(self.device))
-        with torch.cuda.graph(g, stream=main):
-            for s in self.streams:
-                s.wait_stream(main)
-            for i in range(len(self.plans)):
-                with torch.cuda.stream(self.streams[i % len(self.streams)]):
-                    outs[i] = self._call(kind, i)
-            for s in self.streams:
-                main.wait_stream(s)
+        if self.mode == "persistent":
+            with torch.cuda.graph(g, stream=main):
+                outs = self._call_batch(kind)
+        else:
+            outs = [None] * len(self.plans)
+            with torch.cuda.graph(g, stream=main):
+                for s in self.streams:
+                    s.wait_stream(main)
+                for i in range(len(self.plans)):
+                    with torch.cuda.stream(self.streams[i % len(self.streams)]):
+                        outs[i] = self._call_one(kind, i)
+                for s in self.streams:
+                    main.wait_stream(s)
         torch.cuda.current_stream(self.device).wait_stream(main)
         self._graphs[kind] = g
         self._outs[kind] = outs
@@ -188,7 +260,7 @@ class BatchedOperator:
 
     def plain(self, kind: str) -> list:
         """The same work as a plain per-instance loop on one stream."""
-        return [self._call(kind, i) for i in range(len(self.plans))]
+        return [self._call_one(kind, i) for i in range(len(self.plans))]
 
 
 # --------------------------------------------------------------------------

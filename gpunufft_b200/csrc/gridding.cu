@@ -1,20 +1,23 @@
 // Per-call kernels of the operator path (sm_100a).
 //
-// Adjoint ("owner" spread): one CTA per owner sector.  The CTA accumulates
-// the sector's sw^d interior cells for a group of CG coils in shared memory
-// from every sample whose footprint reaches them (its own samples and the
-// boundary samples of neighbouring sectors, listed at plan time), then
-// writes each owned grid cell exactly once with coalesced stores.  No grid
-// memset, no global atomics (except for the few targets whose candidate list
-// is split over several CTAs), no halo write-back.  Warp lanes map to coils,
-// so the footprint arithmetic of a sample is done once per warp and the
-// shared-memory updates of a sample are 32 consecutive float2.
+// Adjoint: the sorted k-space is gathered coil-interleaved (one row of coil
+// values per sample), then spread as a sparse product with the plan's
+// interpolation matrix: one block per grid row chunk and coil group streams
+// the chunk's nonzeros in equal shares per unit of lanes, keeps running
+// cell sums in registers and finishes cells cut by share boundaries in
+// unit order (deterministic, no atomics).  On power-of-two grids the spread
+// takes whole rows and runs the inverse x transform in place before writing
+// only the cropped outputs (k_adjoint_spmm_xfft).
 //
-// Forward: one CTA per (sector, sample slice) gathers the sector tile plus
-// halo for CG coils into shared memory (wrap-around and the upstream's
-// FORWARD fftshift folded into the gather), then each warp interpolates
-// samples with lanes over coils and scatters scaled results straight to the
-// original sample order.
+// Forward: one block per work item (<= 512 samples of one sector) stages the
+// sector tile plus halo of a coil group in shared memory -- by tensor copies
+// when the grid holds the FORWARD-shifted spectrum and the tile is a box of
+// it, else by cp.async gathers with wrap-around and shift folded in -- and
+// interpolates the item's samples, scattering scaled results straight to
+// the original sample order.
+//
+// Batches: every stage above, and the elementwise prepare / finish, as one
+// persistent launch over the (instance, unit) lists of many operators.
 //
 // Upstream references are relative to the upstream CUDA/ directory.
 #include "gridding.cuh"
@@ -115,18 +118,18 @@ __global__ void __launch_bounds__(kThreads)
 
 // The same gather driven by the original order: a block reads 64
 // consecutive original samples of 32 coils (coalesced per coil), and writes
-// each sample's coil row (contiguous) to its sorted position inv[j].
-__global__ void __launch_bounds__(kThreads)
-    k_gather_kspace_inv(const float2 *__restrict__ kspace,
-                        const uint32_t *__restrict__ inv,
-                        const float *__restrict__ dens, uint32_t M, int C,
-                        int CP, float2 *__restrict__ ks)
+// each sample's coil row (contiguous) to its sorted position inv[j].  One
+// unit: sample block jb, coil block cb.
+__device__ __forceinline__ void gather_inv_unit(
+    int jb, int cb, const float2 *__restrict__ kspace,
+    const uint32_t *__restrict__ inv, const float *__restrict__ dens,
+    uint32_t M, int C, int CP, float2 *__restrict__ ks)
 {
   __shared__ float2 tile[kGatherSamples][kGatherCoils + 1];
   __shared__ uint32_t s_t[kGatherSamples];
   __shared__ float sd[kGatherSamples];
-  const size_t j0 = (size_t)blockIdx.x * kGatherSamples;
-  const int c0 = blockIdx.y * kGatherCoils;
+  const size_t j0 = (size_t)jb * kGatherSamples;
+  const int c0 = cb * kGatherCoils;
   const int nc = min(kGatherCoils, CP - c0);
   for (int i = threadIdx.x; i < kGatherSamples; i += kThreads)
   {
@@ -160,6 +163,15 @@ __global__ void __launch_bounds__(kThreads)
       ks[(size_t)s_t[jl] * CP + c0 + cl] = v;
     }
   }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_gather_kspace_inv(const float2 *__restrict__ kspace,
+                        const uint32_t *__restrict__ inv,
+                        const float *__restrict__ dens, uint32_t M, int C,
+                        int CP, float2 *__restrict__ ks)
+{
+  gather_inv_unit(blockIdx.x, blockIdx.y, kspace, inv, dens, M, C, CP, ks);
 }
 
 __global__ void k_invert(const uint32_t *__restrict__ idx, uint32_t M,
@@ -472,24 +484,38 @@ __device__ __forceinline__ void spmm_accumulate(
 }
 
 // V coils per lane (V = 2 reads a lane's two coils as one 16-byte load and
-// halves the per-entry instructions per coil).
-template <int CG, int V>
-__global__ void __launch_bounds__(kThreads, 3)
-    k_adjoint_spmm(const uint32_t *__restrict__ row_off,
-                   const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
-                   int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
+// halves the per-entry instructions per coil).  One unit: grid row
+// (y + G1 * z), chunk of kSpmmCells cells along x, coil group.  Shared
+// memory (SpmmSmem): acc [kSpmmCells][CG + 1], offsets [kSpmmCells + 1],
+// the cut cells' partial sums [NU][CG] and cell indices [NU] x 2.
+template <int CG, int V> struct SpmmSmem
 {
-  constexpr int NU = kWarps * (32 / (CG / V));  // streaming units
-  __shared__ float2 acc_s[kSpmmCells][CG + 1];
-  __shared__ uint32_t s_off[kSpmmCells + 1];
+  static constexpr int NU = kWarps * (32 / (CG / V));  // streaming units
+  static constexpr size_t acc = 0;
+  static constexpr size_t part = acc + (size_t)kSpmmCells * (CG + 1) * 8;
+  static constexpr size_t off = part + (size_t)NU * CG * 8;
+  static constexpr size_t cells = off + ((kSpmmCells + 1) * 4 + 7) / 8 * 8;
+  static constexpr size_t bytes = cells + (size_t)2 * NU * 4;
+};
+
+template <int CG, int V>
+__device__ __forceinline__ void adjoint_spmm_unit(
+    int row, int chunk, int group, const uint32_t *__restrict__ row_off,
+    const uint2 *__restrict__ nz, const float2 *__restrict__ ks, int CP,
+    const Geo &g, int C, int shift, float2 *__restrict__ grid,
+    unsigned char *sm)
+{
+  using L = SpmmSmem<CG, V>;
+  constexpr int NU = L::NU;
+  float2 *acc_s = reinterpret_cast<float2 *>(sm + L::acc);
+  uint32_t *s_off = reinterpret_cast<uint32_t *>(sm + L::off);
   // cells cut by share boundaries: head = the partial sum of the unit's
   // first cell when it started in an earlier share, tail = its last cell
   // when it started in this share and continues in the next
-  __shared__ float2 part_head[NU][CG];
-  __shared__ int head_cell[NU], tail_cell[NU];
-  const int x0 = blockIdx.y * kSpmmCells;
-  const int row = blockIdx.x;  // y + G1 * z
-  const int group = blockIdx.z;
+  float2 *part_head = reinterpret_cast<float2 *>(sm + L::part);
+  int *head_cell = reinterpret_cast<int *>(sm + L::cells);
+  int *tail_cell = head_cell + NU;
+  const int x0 = chunk * kSpmmCells;
   const int nxc = min(kSpmmCells, g.G[0] - x0);
   const long long rowbase = (long long)row * g.G[0] + x0;
   for (int i = threadIdx.x; i <= nxc; i += kThreads)
@@ -520,14 +546,13 @@ __global__ void __launch_bounds__(kThreads, 3)
     return;
   }
   for (int i = threadIdx.x; i < kSpmmCells * (CG + 1); i += kThreads)
-    (&acc_s[0][0])[i] = make_float2(0.f, 0.f);
+    acc_s[i] = make_float2(0.f, 0.f);
   for (int i = threadIdx.x; i < NU; i += kThreads)
     head_cell[i] = tail_cell[i] = -1;
   __syncthreads();
 
-  spmm_accumulate<CG, V>(s_off, nxc, nz, ks, CP, group, &acc_s[0][0],
-                         &part_head[0][0], head_cell,
-                         tail_cell);
+  spmm_accumulate<CG, V>(s_off, nxc, nz, ks, CP, group, acc_s, part_head,
+                         head_cell, tail_cell);
   __syncthreads();
   for (int idx = threadIdx.x; idx < CG * kSpmmCells; idx += kThreads)
   {
@@ -538,8 +563,19 @@ __global__ void __launch_bounds__(kThreads, 3)
     int x = x0 + xi;
     if (shift)
       x = wrap_mod(x - g.shift_inv[0], g.G[0]);
-    grid[(long long)c * g.grid_count + orow + x] = acc_s[xi][cl];
+    grid[(long long)c * g.grid_count + orow + x] = acc_s[xi * (CG + 1) + cl];
   }
+}
+
+template <int CG, int V>
+__global__ void __launch_bounds__(kThreads, 3)
+    k_adjoint_spmm(const uint32_t *__restrict__ row_off,
+                   const uint2 *__restrict__ nz, const float2 *__restrict__ ks,
+                   int CP, Geo g, int C, int shift, float2 *__restrict__ grid)
+{
+  __shared__ __align__(16) unsigned char sm[SpmmSmem<CG, V>::bytes];
+  adjoint_spmm_unit<CG, V>(blockIdx.x, blockIdx.y, blockIdx.z, row_off, nz,
+                           ks, CP, g, C, shift, grid, sm);
 }
 
 // --------------------------------------------------------------------------
@@ -767,22 +803,20 @@ __global__ void __launch_bounds__(kThreads, xfft_min_blocks(CG, L))
 // --------------------------------------------------------------------------
 // Shared memory: [tile: pad^DIM cells x (CG+1) float2][per-sample geometry
 // (DIM ints) and weights (DIM x KS floats)].
-template <int DIM, int CG, int KS>
-__global__ void __launch_bounds__(kThreads)
-    k_forward_interp(const FwdItem *__restrict__ items,
-                     const float *__restrict__ traj,
-                     const uint32_t *__restrict__ idx,
-                     const float *__restrict__ dens,
-                     const float2 *__restrict__ grid, Geo g,
-                     const float *__restrict__ lut, uint32_t M, int C,
-                     int shift, float scale, float2 *__restrict__ out)
+// One unit: work item `it`, coil group `group` of CG coils (a power of two
+// <= 32: lanes per sample; a constant where the caller has one); smem as
+// above.
+template <int DIM, int KS>
+__device__ __forceinline__ void forward_interp_unit(
+    const FwdItem it, int group, const float *__restrict__ traj,
+    const uint32_t *__restrict__ idx, const float *__restrict__ dens,
+    const float2 *__restrict__ grid, const Geo &g,
+    const float *__restrict__ lut, uint32_t M, int C, int shift, float scale,
+    float2 *__restrict__ out, float2 *smem, const int CG)
 {
-  extern __shared__ float2 smem[];
-  constexpr int SLOTS = 32 / CG;
-  constexpr int PITCH = CG + 1;
+  const int SLOTS = 32 / CG;
+  const int PITCH = CG + 1;
   constexpr int CH = kThreads;
-  const FwdItem it = items[blockIdx.x];
-  const int group = blockIdx.y;
   const int pad = g.pad;
   const int tcells = DIM == 3 ? pad * pad * pad : pad * pad;
   float2 *tile = smem;
@@ -951,6 +985,22 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
   }
+}
+
+template <int DIM, int CG, int KS>
+__global__ void __launch_bounds__(kThreads)
+    k_forward_interp(const FwdItem *__restrict__ items,
+                     const float *__restrict__ traj,
+                     const uint32_t *__restrict__ idx,
+                     const float *__restrict__ dens,
+                     const float2 *__restrict__ grid, Geo g,
+                     const float *__restrict__ lut, uint32_t M, int C,
+                     int shift, float scale, float2 *__restrict__ out)
+{
+  extern __shared__ float2 smem[];
+  forward_interp_unit<DIM, KS>(items[blockIdx.x], blockIdx.y, traj, idx, dens,
+                               grid, g, lut, M, C, shift, scale, out, smem,
+                               CG);
 }
 
 // --------------------------------------------------------------------------
@@ -1406,16 +1456,17 @@ __global__ void __launch_bounds__(kThreads, MINB)
 // --------------------------------------------------------------------------
 // image-space stages
 // --------------------------------------------------------------------------
+// Image pixel p of the adjoint from the transformed grid.
 template <bool SENS>
-__global__ void k_adjoint_finish(const float2 *__restrict__ grid,
-                                 const float *__restrict__ deapo,
-                                 const float2 *__restrict__ sens, Geo g, int C,
-                                 int stage, int accumulate,
-                                 float2 *__restrict__ out)
+__device__ __forceinline__ void finish_pixel(long long p,
+                                             const float2 *__restrict__ grid,
+                                             const float *__restrict__ deapo,
+                                             const float2 *__restrict__ sens,
+                                             const Geo &g, int C, int stage,
+                                             int accumulate,
+                                             float2 *__restrict__ out)
 {
   const long long N = g.img_count, G = g.grid_count;
-  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < N;
-       p += (long long)gridDim.x * blockDim.x)
   {
     const int x = (int)(p % g.N[0]);
     const int y = (int)((p / g.N[0]) % g.N[1]);
@@ -1466,6 +1517,18 @@ __global__ void k_adjoint_finish(const float2 *__restrict__ grid,
   }
 }
 
+template <bool SENS>
+__global__ void k_adjoint_finish(const float2 *__restrict__ grid,
+                                 const float *__restrict__ deapo,
+                                 const float2 *__restrict__ sens, Geo g, int C,
+                                 int stage, int accumulate,
+                                 float2 *__restrict__ out)
+{
+  for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+       p < g.img_count; p += (long long)gridDim.x * blockDim.x)
+    finish_pixel<SENS>(p, grid, deapo, sens, g, C, stage, accumulate, out);
+}
+
 // Each block handles grid rows (coil, z, y) with threads along x, two
 // cells per thread (16-byte stores).  Rows whose (shifted) position falls
 // outside the zero-padded image are pure zero stores.
@@ -1498,13 +1561,13 @@ __device__ __forceinline__ float2 prepare_value(const float2 *__restrict__ image
 // is multiplied by (-1)^(x+y+z): the transform then yields the spectrum
 // FORWARD-shifted by G/2 = ceil(G/2) on every axis, whose sector tiles are
 // boxes of the grid.
+// One unit: rows yb * rpb .. of plane z of coil c.
 template <bool SENS>
-__global__ void __launch_bounds__(kThreads)
-    k_forward_prepare(const float2 *__restrict__ image,
-                      const float2 *__restrict__ sens,
-                      const float *__restrict__ deapo, Geo g, int c0,
-                      int image_grid, int signs, int tpr,
-                      float2 *__restrict__ grid)
+__device__ __forceinline__ void prepare_unit(
+    int yb, int z, int c, const float2 *__restrict__ image,
+    const float2 *__restrict__ sens, const float *__restrict__ deapo,
+    const Geo &g, int image_grid, int signs, int tpr,
+    float2 *__restrict__ grid)
 {
   const int X = image_grid ? g.N[0] : g.G[0];
   const int Y = image_grid ? g.N[1] : g.G[1];
@@ -1515,9 +1578,7 @@ __global__ void __launch_bounds__(kThreads)
   const bool vec = (X & 1) == 0;
   const int rpb = kThreads / tpr;  // rows per block
   const int lr = threadIdx.x / tpr, lt = threadIdx.x - lr * tpr;
-  const int y = blockIdx.x * rpb + lr;
-  const int z = blockIdx.y;
-  const int c = c0 + blockIdx.z;
+  const int y = yb * rpb + lr;
   if (lr >= rpb || y >= Y)
     return;
   float2 *dst = grid + (long long)c * plane + ((long long)z * Y + y) * X;
@@ -1600,6 +1661,18 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+template <bool SENS>
+__global__ void __launch_bounds__(kThreads)
+    k_forward_prepare(const float2 *__restrict__ image,
+                      const float2 *__restrict__ sens,
+                      const float *__restrict__ deapo, Geo g, int c0,
+                      int image_grid, int signs, int tpr,
+                      float2 *__restrict__ grid)
+{
+  prepare_unit<SENS>(blockIdx.x, blockIdx.y, c0 + blockIdx.z, image, sens,
+                     deapo, g, image_grid, signs, tpr, grid);
+}
+
 template <typename K>
 void set_smem(K kernel, size_t bytes)
 {
@@ -1634,6 +1707,193 @@ int pow2_at_least(int c)
 
 // footprint slots per axis: kw + 1 cells
 int slots_for(const Geo &g) { return g.kw + 1 <= 4 ? 4 : 8; }
+
+// --------------------------------------------------------------------------
+// batches: one persistent launch per stage over all instances
+// --------------------------------------------------------------------------
+// Copies instance i's descriptor into shared memory (all threads; a
+// barrier follows) unless it is already there.
+__device__ __forceinline__ void batch_load(const BatchInst *__restrict__ inst,
+                                           int i, BatchInst *s_b, int *s_cur)
+{
+  if (*s_cur == i)
+    return;
+  constexpr int W = (int)(sizeof(BatchInst) / 4);
+  const uint32_t *src = reinterpret_cast<const uint32_t *>(inst + i);
+  uint32_t *dst = reinterpret_cast<uint32_t *>(s_b);
+  __syncthreads();
+  for (int k = threadIdx.x; k < W; k += kThreads)
+    dst[k] = __ldg(src + k);
+  __syncthreads();
+  if (threadIdx.x == 0)
+    *s_cur = i;  // read again only after the next unit's barriers
+}
+
+// The unit loop of a batch stage: thread 0 takes the next unit index from
+// the counter, the block finds its instance (last one whose first unit is
+// <= the index) and runs body(instance, unit within the instance) with the
+// descriptor in shared memory.  Ends when the counter passes `total`.
+template <class F>
+__device__ __forceinline__ void batch_loop(const BatchInst *__restrict__ inst,
+                                           int n, int stage, uint32_t total,
+                                           unsigned *counter, F body)
+{
+  __shared__ uint32_t s_first[kBatchMax + 1];
+  __shared__ uint32_t s_u;
+  __shared__ int s_cur;
+  __shared__ BatchInst s_b;
+  for (int i = threadIdx.x; i < n; i += kThreads)
+    s_first[i] = __ldg(&inst[i].first[stage]);
+  if (threadIdx.x == 0)
+  {
+    s_first[n] = total;
+    s_cur = -1;
+  }
+  for (;;)
+  {
+    __syncthreads();  // the previous unit is done with shared memory
+    if (threadIdx.x == 0)
+      s_u = atomicAdd(counter, 1u);
+    __syncthreads();
+    const uint32_t u = s_u;
+    if (u >= total)
+      return;
+    int lo = 0, hi = n;  // s_first[lo] <= u < s_first[hi]
+    while (hi - lo > 1)
+    {
+      const int mid = (lo + hi) >> 1;
+      if (s_first[mid] <= u)
+        lo = mid;
+      else
+        hi = mid;
+    }
+    batch_load(inst, lo, &s_b, &s_cur);
+    body(lo, u - s_first[lo], s_b);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_prepare(const BatchInst *__restrict__ inst, int n, uint32_t total,
+                    unsigned *counter, const __grid_constant__ BatchIo io)
+{
+  batch_loop(inst, n, kBatchPrepare, total, counter,
+             [&](int i, uint32_t u, const BatchInst &b) {
+               const int rpb = kThreads / b.tpr;
+               const uint32_t nyb = (b.g.G[1] + rpb - 1) / rpb;
+               const uint32_t Z = b.g.G[2];
+               const int yb = (int)(u % nyb), z = (int)((u / nyb) % Z);
+               const int c = (int)(u / (nyb * Z));
+               if (b.sens)
+                 prepare_unit<true>(yb, z, c, io.in[i], b.sens, b.deapo, b.g,
+                                    0, b.signs, b.tpr, b.grid);
+               else
+                 prepare_unit<false>(yb, z, c, io.in[i], nullptr, b.deapo,
+                                     b.g, 0, b.signs, b.tpr, b.grid);
+             });
+}
+
+template <int DIM, int KS>
+__device__ __forceinline__ void batch_interp_unit(const BatchInst &b,
+                                                  uint32_t u, float2 *out,
+                                                  float2 *smem)
+{
+  const uint32_t ng = (b.C + b.fwd_cg - 1) / b.fwd_cg;
+  forward_interp_unit<DIM, KS>(b.items[u / ng], (int)(u % ng), b.traj, b.di,
+                               b.dens, b.grid, b.g, b.lut, b.M, b.C,
+                               b.signs ? 0 : 1, b.g.fft_scale, out, smem,
+                               b.fwd_cg);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_interp(const BatchInst *__restrict__ inst, int n, uint32_t total,
+                   unsigned *counter, const __grid_constant__ BatchIo io)
+{
+  extern __shared__ float2 smem[];
+  batch_loop(inst, n, kBatchInterp, total, counter,
+             [&](int i, uint32_t u, const BatchInst &b) {
+               float2 *out = io.out[i];
+               if (b.g.dim == 3)
+               {
+                 if (b.slots == 4)
+                   batch_interp_unit<3, 4>(b, u, out, smem);
+                 else
+                   batch_interp_unit<3, 8>(b, u, out, smem);
+               }
+               else if (b.slots == 4)
+                 batch_interp_unit<2, 4>(b, u, out, smem);
+               else
+                 batch_interp_unit<2, 8>(b, u, out, smem);
+             });
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_gather(const BatchInst *__restrict__ inst, int n, uint32_t total,
+                   unsigned *counter, const __grid_constant__ BatchIo io)
+{
+  batch_loop(inst, n, kBatchGather, total, counter,
+             [&](int i, uint32_t u, const BatchInst &b) {
+               const uint32_t nj = (b.M + kGatherSamples - 1) / kGatherSamples;
+               gather_inv_unit((int)(u % nj), (int)(u / nj), io.in[i],
+                               b.di_inv, b.dens, b.M, b.C, b.CP, b.ks);
+             });
+}
+
+__host__ __device__ constexpr size_t batch_spread_smem()
+{
+  size_t m = SpmmSmem<1, 1>::bytes;
+  m = m > SpmmSmem<2, 1>::bytes ? m : SpmmSmem<2, 1>::bytes;
+  m = m > SpmmSmem<4, 2>::bytes ? m : SpmmSmem<4, 2>::bytes;
+  m = m > SpmmSmem<8, 2>::bytes ? m : SpmmSmem<8, 2>::bytes;
+  m = m > SpmmSmem<16, 2>::bytes ? m : SpmmSmem<16, 2>::bytes;
+  m = m > SpmmSmem<32, 2>::bytes ? m : SpmmSmem<32, 2>::bytes;
+  return m;
+}
+
+__global__ void __launch_bounds__(kThreads, 3)
+    k_batch_spread(const BatchInst *__restrict__ inst, int n, uint32_t total,
+                   unsigned *counter)
+{
+  __shared__ __align__(16) unsigned char sm[batch_spread_smem()];
+  batch_loop(inst, n, kBatchSpread, total, counter,
+             [&](int, uint32_t u, const BatchInst &b) {
+               const uint32_t rows = (uint32_t)b.g.G[1] * b.g.G[2];
+               const uint32_t nch = (b.g.G[0] + kSpmmCells - 1) / kSpmmCells;
+               const int row = (int)(u % rows);
+               const int ch = (int)((u / rows) % nch);
+               const int grp = (int)(u / (rows * nch));
+#define GN_BSPMM(CGV, VV)                                                      \
+  adjoint_spmm_unit<CGV, VV>(row, ch, grp, b.w_rows, b.w_nz, b.ks, b.CP, b.g,  \
+                             b.C, 1, b.grid, sm)
+               switch (b.spmm_cg)
+               {
+               case 1: GN_BSPMM(1, 1); break;
+               case 2: GN_BSPMM(2, 1); break;
+               case 4: GN_BSPMM(4, 2); break;
+               case 8: GN_BSPMM(8, 2); break;
+               case 16: GN_BSPMM(16, 2); break;
+               default: GN_BSPMM(32, 2); break;
+               }
+#undef GN_BSPMM
+             });
+}
+
+__global__ void __launch_bounds__(kThreads)
+    k_batch_finish(const BatchInst *__restrict__ inst, int n, uint32_t total,
+                   unsigned *counter, const __grid_constant__ BatchIo io)
+{
+  batch_loop(inst, n, kBatchFinish, total, counter,
+             [&](int i, uint32_t u, const BatchInst &b) {
+               const long long p = (long long)u * kThreads + threadIdx.x;
+               if (p >= b.g.img_count)
+                 return;
+               if (b.sens)
+                 finish_pixel<true>(p, b.grid, b.deapo, b.sens, b.g, b.C, 2,
+                                    0, io.out[i]);
+               else
+                 finish_pixel<false>(p, b.grid, b.deapo, nullptr, b.g, b.C, 2,
+                                     0, io.out[i]);
+             });
+}
 }  // namespace
 
 int spmm_coil_group(int C) { return C > 16 ? 32 : pow2_at_least(C); }
@@ -2120,6 +2380,106 @@ bool launch_adjoint_spmm_xfft(const uint32_t *row_off, const uint2 *nz,
     return false;
   GN_LAUNCH_CHECK("adjoint spread with x transform");
   return true;
+}
+
+// --------------------------------------------------------------------------
+// batches (host side)
+// --------------------------------------------------------------------------
+void batch_configure(BatchInst &b, int tile_coils)
+{
+  const Geo &g = b.g;
+  b.spmm_cg = spmm_coil_group(b.C);
+  b.CP = (b.C + b.spmm_cg - 1) / b.spmm_cg * b.spmm_cg;
+  b.slots = slots_for(g);
+  int cg = forward_coil_group(b.C, g.dim, g.pad);
+  if (tile_coils > 0)
+    cg = tile_coils > 32 ? 32 : pow2_at_least(tile_coils);
+  if (g.dim == 3 && cg > 8)
+    cg = 8;
+  // tiles within 72 KB keep three blocks of the interpolation stage per SM
+  while (cg > 1 && forward_smem_bytes(g, cg) > 72 * 1024)
+    cg >>= 1;
+  b.fwd_cg = cg;
+  const int X = g.G[0];
+  const int work = (X & 1) == 0 ? X / 2 : X;
+  b.tpr = work >= 64 ? 64 : (work > 0 ? work : 1);
+}
+
+void batch_units(const BatchInst &b, uint32_t units[kBatchStages])
+{
+  const Geo &g = b.g;
+  const uint32_t rpb = kThreads / b.tpr;
+  units[kBatchPrepare] =
+      (uint32_t)((g.G[1] + rpb - 1) / rpb) * g.G[2] * (uint32_t)b.C;
+  units[kBatchInterp] =
+      (uint32_t)b.n_items * (uint32_t)((b.C + b.fwd_cg - 1) / b.fwd_cg);
+  units[kBatchGather] = (uint32_t)((b.M + kGatherSamples - 1) / kGatherSamples) *
+                        (uint32_t)((b.CP + kGatherCoils - 1) / kGatherCoils);
+  units[kBatchSpread] =
+      (uint32_t)g.G[1] * g.G[2] *
+      (uint32_t)((g.G[0] + kSpmmCells - 1) / kSpmmCells) *
+      (uint32_t)((b.C + b.spmm_cg - 1) / b.spmm_cg);
+  units[kBatchFinish] = (uint32_t)((g.img_count + kThreads - 1) / kThreads);
+}
+
+size_t batch_interp_smem(const BatchInst &b)
+{
+  return forward_smem_bytes(b.g, b.fwd_cg);
+}
+
+namespace
+{
+// persistent blocks: as many as are resident on the device at once
+template <typename K>
+unsigned resident_blocks(K kernel, size_t smem)
+{
+  int dev = 0, sms = 0, per_sm = 0;
+  GN_CUDA(cudaGetDevice(&dev));
+  GN_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel,
+                                                        kThreads, smem));
+  return (unsigned)std::max(1, sms * std::max(1, per_sm));
+}
+}  // namespace
+
+unsigned launch_batch_stage(int stage, const BatchInst *inst, int n,
+                            uint32_t total, const BatchIo *io,
+                            unsigned *counter, size_t interp_smem,
+                            cudaStream_t s)
+{
+  if (total == 0 || n <= 0)
+    return 0;
+  if (n > kBatchMax)
+    throw Error(kInvalidArgument, "too many instances in a batch");
+  unsigned nb = 0;
+  switch (stage)
+  {
+  case kBatchPrepare:
+    nb = std::min<unsigned>(total, resident_blocks(k_batch_prepare, 0));
+    k_batch_prepare<<<nb, kThreads, 0, s>>>(inst, n, total, counter, *io);
+    break;
+  case kBatchInterp:
+    set_smem(k_batch_interp, interp_smem);
+    nb = std::min<unsigned>(total,
+                            resident_blocks(k_batch_interp, interp_smem));
+    k_batch_interp<<<nb, kThreads, interp_smem, s>>>(inst, n, total, counter,
+                                                     *io);
+    break;
+  case kBatchGather:
+    nb = std::min<unsigned>(total, resident_blocks(k_batch_gather, 0));
+    k_batch_gather<<<nb, kThreads, 0, s>>>(inst, n, total, counter, *io);
+    break;
+  case kBatchSpread:
+    nb = std::min<unsigned>(total, resident_blocks(k_batch_spread, 0));
+    k_batch_spread<<<nb, kThreads, 0, s>>>(inst, n, total, counter);
+    break;
+  default:
+    nb = std::min<unsigned>(total, resident_blocks(k_batch_finish, 0));
+    k_batch_finish<<<nb, kThreads, 0, s>>>(inst, n, total, counter, *io);
+    break;
+  }
+  GN_LAUNCH_CHECK("batch stage");
+  return nb;
 }
 
 }  // namespace gnufft

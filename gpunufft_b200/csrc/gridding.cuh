@@ -125,4 +125,70 @@ void build_forward_lane_order(const FwdItem *items, int n_items,
 // reads it).
 bool forward_pairs(const Geo &g, int tile_coils);
 
+// --------------------------------------------------------------------------
+// Batches of independent operators: every stage of all instances in one
+// launch.  Each stage is a list of work units (instance, unit) with the
+// instances' units consecutive; persistent blocks take unit indices from a
+// counter (atomicAdd, no waiting) and run the unit with the template
+// configuration of its instance.  The transforms between the stages are
+// one cuFFT call per instance.
+// --------------------------------------------------------------------------
+constexpr int kBatchMax = 512;
+enum BatchStage
+{
+  kBatchPrepare = 0,  // S x, deapodization, pad, shift (forward)
+  kBatchInterp,       // interpolation to the samples (forward)
+  kBatchGather,       // k-space to sorted, coil-interleaved order (adjoint)
+  kBatchSpread,       // interpolation matrix x k-space into the grid
+  kBatchFinish,       // crop, scale, deapodization, conj(S) coil sum
+  kBatchStages
+};
+
+struct BatchInst
+{
+  Geo g;
+  uint32_t M;
+  int C;        // coils of the instance
+  int CP;       // coil lanes of the sorted k-space (multiple of spmm_cg)
+  int spmm_cg;  // coils per spread group
+  int fwd_cg;   // coils per forward tile
+  int slots;    // footprint slots per axis (4 or 8)
+  int signs;    // grid cells multiplied by (-1)^(x+y+z) before the forward
+                // transform (grids even along every axis)
+  int tpr;      // prepare: threads per grid row
+  int n_items;
+  const FwdItem *items;
+  const float *traj, *dens, *lut, *deapo;
+  const uint32_t *di, *di_inv, *w_rows;
+  const uint2 *w_nz;
+  const float2 *sens;  // coil maps [C][N] (coil combine), or NULL
+  float2 *grid;        // scratch [C][G]
+  float2 *ks;          // scratch [M][CP]
+  uint32_t first[kBatchStages];  // the instance's first unit of each stage
+};
+
+// Per-call data pointers of the instances (stage inputs / outputs).
+struct BatchIo
+{
+  const float2 *in[kBatchMax];
+  float2 *out[kBatchMax];
+};
+
+// Fills the configuration fields of `b` (CP, spmm_cg, fwd_cg, slots, tpr)
+// from its geometry and coil count; tile_coils > 0 asks for that forward
+// tile (reduced to fit).
+void batch_configure(BatchInst &b, int tile_coils);
+// Units of each stage for one configured instance.
+void batch_units(const BatchInst &b, uint32_t units[kBatchStages]);
+// Dynamic shared memory of the instance's interpolation units.
+size_t batch_interp_smem(const BatchInst &b);
+// One launch of `stage` over the n instances (device array `inst`, units
+// `total`); `counter` (device, zero before the launch) hands out the units.
+// `io` carries the inputs / outputs of the stages that read or write the
+// caller's data.  Returns the number of blocks launched.
+unsigned launch_batch_stage(int stage, const BatchInst *inst, int n,
+                            uint32_t total, const BatchIo *io,
+                            unsigned *counter, size_t interp_smem,
+                            cudaStream_t s);
+
 }  // namespace gnufft

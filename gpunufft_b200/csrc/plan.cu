@@ -26,6 +26,7 @@
 
 #include "../../include/gpunufft_b200.h"
 #include "binning.cuh"
+#include "capi.hpp"
 #include "devutil.hpp"
 #include "fftpass.cuh"
 #include "footprint.cuh"
@@ -55,12 +56,6 @@ struct SectorPair
 
 const char *kVersion = "gpunufft_b200 0.1.0 (sm_100a)";
 
-void check_cufft(cufftResult r, const char *what)
-{
-  if (r != CUFFT_SUCCESS)
-    throw Error(r == CUFFT_ALLOC_FAILED ? kOutOfMemory : kCufftError,
-                std::string(what) + ": cuFFT error " + std::to_string((int)r));
-}
 }  // namespace
 
 struct gnufft_plan
@@ -190,51 +185,6 @@ struct gnufft_plan
 
 namespace
 {
-int fail(int st, const std::string &msg)
-{
-  g_last_error = msg;
-  return st;
-}
-
-template <class F> gnufft_status guarded(F &&f)
-{
-  try
-  {
-    f();
-    return GNUFFT_SUCCESS;
-  }
-  catch (const Error &e)
-  {
-    g_last_error = e.what();
-    return (gnufft_status)e.status;
-  }
-  catch (const std::bad_alloc &)
-  {
-    g_last_error = "host allocation failed";
-    return GNUFFT_ERROR_OUT_OF_MEMORY;
-  }
-  catch (const std::exception &e)
-  {
-    g_last_error = e.what();
-    return GNUFFT_ERROR_INTERNAL;
-  }
-}
-
-struct DeviceGuard
-{
-  int prev = -1;
-  explicit DeviceGuard(int dev)
-  {
-    cudaGetDevice(&prev);
-    GN_CUDA(cudaSetDevice(dev));
-  }
-  ~DeviceGuard()
-  {
-    if (prev >= 0)
-      cudaSetDevice(prev);
-  }
-};
-
 template <class T> void upload(DeviceBuffer &b, const T *h, size_t n,
                                cudaStream_t s)
 {
@@ -1048,6 +998,30 @@ bool plan_view(const gnufft_plan *p, PlanView *v)
   v->dens_sorted = p->has_dens ? p->dens_sorted.as<float>() : nullptr;
   v->w_rows = p->w_rows.as<uint32_t>();
   v->w_nz = p->w_nz.as<uint2>();
+  return true;
+}
+
+bool plan_tables(gnufft_plan *p, uint32_t n_coils, PlanTables *t)
+{
+  if (!p || !t)
+    return false;
+  t->g = p->g;
+  t->M = p->M;
+  t->device = p->desc.device;
+  t->sens_coils = p->sens_coils;
+  t->tile_coils = p->fwd_tile_coils;
+  t->items = p->fwd_items.as<FwdItem>();
+  t->n_items = p->n_fwd_items;
+  t->traj_sorted = p->traj_sorted.as<float>();
+  t->dens_sorted = p->has_dens ? p->dens_sorted.as<float>() : nullptr;
+  t->lut = p->lut.as<float>();
+  t->deapo = p->deapo.as<float>();
+  t->data_indices = p->di.as<uint32_t>();
+  t->inverse_indices = p->di_inv.as<uint32_t>();
+  t->w_rows = p->w_rows.as<uint32_t>();
+  t->w_nz = p->w_nz.as<uint2>();
+  t->sens = p->sens_coils ? p->sens.as<float2>() : nullptr;
+  t->fft = p->fft_plan((int)n_coils);
   return true;
 }
 

@@ -6,8 +6,10 @@
 #include <string>
 
 #include <cuda_runtime.h>
+#include <cufft.h>
 
 #include "geometry.hpp"
+#include "gridding.cuh"
 
 struct gnufft_plan;
 
@@ -28,6 +30,27 @@ struct PlanView
 
 // Fill `v` from `p`; false if `p` is NULL.
 bool plan_view(const gnufft_plan *p, PlanView *v);
+
+// What a batch of operators reads from one plan: its resident tables, its
+// maps (when it has maps for n_coils channels) and its cuFFT plan for
+// n_coils transforms of the grid (created on first use; the plan's device
+// must be current).
+struct PlanTables
+{
+  Geo g;
+  uint32_t M;
+  int device;
+  uint32_t sens_coils;
+  int tile_coils;  // forward tile coils asked for at creation (0: automatic)
+  const FwdItem *items;
+  int n_items;
+  const float *traj_sorted, *dens_sorted, *lut, *deapo;
+  const uint32_t *data_indices, *inverse_indices, *w_rows;
+  const uint2 *w_nz;
+  const float2 *sens;  // NULL without maps
+  cufftHandle fft;
+};
+bool plan_tables(gnufft_plan *p, uint32_t n_coils, PlanTables *t);
 
 // Set the message returned by gnufft_last_error() for this thread.
 void set_last_error(const std::string &msg);

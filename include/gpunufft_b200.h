@@ -302,6 +302,57 @@ GNUFFT_API gnufft_status gnufft_plan_check(gnufft_plan *plan);
 GNUFFT_API gnufft_status gnufft_get_stage_times(const gnufft_plan *plan,
                                      gnufft_stage_times *times);
 
+/* Batches of independent operators (no counterpart in the upstream, whose
+ * operators each run their own per-coil loop).  A batch runs the full
+ * operator (DEAPODIZATION output: coil combine when the plan has maps) of
+ * many instances -- different trajectories, image sizes, oversampling,
+ * kernel widths, sector widths and coil counts -- with every gridding
+ * stage of all instances in one persistent launch: forward = prepare
+ * (maps, deapodization, pad, shift), one cuFFT call per instance,
+ * interpolation; adjoint = k-space gather, spread, one cuFFT call per
+ * instance, finish (crop, deapodization, conj(maps) coil sum).  Each stage's
+ * blocks take (instance, work item) units from a device counter.
+ *
+ * gnufft_batch_create: plans[i] and n_coils[i] describe instance i (n_coils
+ * must equal the plan's map channels when it has maps); one plan may appear
+ * several times (frames sharing a trajectory).  All plans on one device;
+ * they must outlive the batch, and their maps must not be replaced with a
+ * different channel count while it exists.  The batch owns the instances'
+ * scratch (grid and sorted k-space).  At most 512 instances.
+ *
+ * gnufft_batch_forward: images[i] (device): [n_coils][image] complex64, or
+ * [image] when the plan has maps; kspace[i] (device, output):
+ * [n_coils][M] in original sample order.  gnufft_batch_adjoint: the
+ * reverse.  Calls are ordered on `stream` and may be captured into a CUDA
+ * graph; a batch is not reentrant. */
+typedef struct gnufft_batch gnufft_batch;
+typedef struct
+{
+  uint32_t n_instances;
+  uint32_t units[5];       /* work units per stage: prepare, interpolation,
+                              gather, spread, finish */
+  uint32_t kernels_forward; /* this library's launches per forward */
+  uint32_t kernels_adjoint; /* ... per adjoint (cuFFT calls not counted) */
+  uint32_t fft_calls;       /* cuFFT calls per forward or adjoint */
+  uint64_t device_bytes;    /* scratch and descriptors owned by the batch */
+} gnufft_batch_info;
+
+GNUFFT_API gnufft_status gnufft_batch_create(gnufft_plan *const *plans,
+                                             const uint32_t *n_coils,
+                                             uint32_t n_instances,
+                                             gnufft_batch **out);
+GNUFFT_API gnufft_status gnufft_batch_forward(gnufft_batch *batch,
+                                              const void *const *images,
+                                              void *const *kspace,
+                                              void *stream);
+GNUFFT_API gnufft_status gnufft_batch_adjoint(gnufft_batch *batch,
+                                              const void *const *kspace,
+                                              void *const *images,
+                                              void *stream);
+GNUFFT_API gnufft_status gnufft_batch_get_info(const gnufft_batch *batch,
+                                               gnufft_batch_info *info);
+GNUFFT_API gnufft_status gnufft_batch_destroy(gnufft_batch *batch);
+
 GNUFFT_API const char *gnufft_last_error(void);
 GNUFFT_API const char *gnufft_status_string(gnufft_status status);
 GNUFFT_API const char *gnufft_version(void);
