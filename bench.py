@@ -859,8 +859,8 @@ def run_batch_arm(args, rank, world):
     b = batch_run(dev, args.steps, args.warmup, seed=rank)
     if rank == 0:
         print(json.dumps({
-            "metric": "uneven batch: instance fwd+adj/s, one CUDA graph vs "
-                      "plain per-instance loop",
+            "metric": "uneven batch: instance fwd+adj/s, persistent batch "
+                      "from a CUDA graph vs plain per-instance loop",
             "value": world * b["value"], "unit": "instances/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": b["ms_per_step"], "higher_is_better": True,
@@ -868,8 +868,9 @@ def run_batch_arm(args, rank, world):
             "data": "synthetic",
             "config": {"workload": b["workload"],
                        "instances": b["instances"]},
-            "plain": b["plain"], "graph_over_plain": b["graph_over_plain"],
-            "autotune": b["autotune"],
+            **{k: b[k] for k in ("launches_per_step", "streams_graph",
+                                 "plain", "graph_over_plain",
+                                 "persistent_over_streams", "autotune")},
         }), flush=True)
 
 

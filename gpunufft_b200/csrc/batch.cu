@@ -30,6 +30,23 @@ struct gnufft_batch
   uint32_t total[kBatchStages] = {};
   size_t interp_smem = 0;
   BatchIo io{};  // per-call data pointers (kernel parameter)
+  // the transforms run on side streams forked from the caller's stream;
+  // instances that share a cuFFT plan (frames of one plan) share a side
+  // stream, since a plan's work area serves one transform at a time
+  std::vector<int> fft_stream;
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> join;
+  cudaEvent_t fork = nullptr;
+
+  ~gnufft_batch()
+  {
+    for (cudaStream_t st : side)
+      cudaStreamDestroy(st);
+    for (cudaEvent_t e : join)
+      cudaEventDestroy(e);
+    if (fork)
+      cudaEventDestroy(fork);
+  }
 };
 
 namespace
@@ -42,14 +59,40 @@ void check_batch(const gnufft_batch *b)
     throw Error(kInvalidArgument, "NULL batch");
 }
 
+constexpr int kSideStreams = 8;
+
+// One cuFFT call per instance, spread over the side streams (fork: the
+// side streams wait for the caller's stream; join: the caller's stream
+// waits for every side stream).  Event records and waits are captured
+// into a CUDA graph like the launches.
 void run_ffts(gnufft_batch &b, int direction, cudaStream_t s)
 {
+  GN_CUDA(cudaEventRecord(b.fork, s));
+  for (cudaStream_t st : b.side)
+    GN_CUDA(cudaStreamWaitEvent(st, b.fork, 0));
   for (uint32_t i = 0; i < b.n; ++i)
   {
-    check_cufft(cufftSetStream(b.fft[i], s), "cufftSetStream");
+    cudaStream_t st = b.side[b.fft_stream[i]];
+    check_cufft(cufftSetStream(b.fft[i], st), "cufftSetStream");
     cufftComplex *g = reinterpret_cast<cufftComplex *>(b.inst[i].grid);
     check_cufft(cufftExecC2C(b.fft[i], g, g, direction), "cufftExecC2C");
   }
+  for (size_t k = 0; k < b.side.size(); ++k)
+  {
+    GN_CUDA(cudaEventRecord(b.join[k], b.side[k]));
+    GN_CUDA(cudaStreamWaitEvent(s, b.join[k], 0));
+  }
+}
+
+// Public work units per stage: prepare, interpolation (2-D and 3-D),
+// gather, spread, finish.
+void public_units(const gnufft_batch &b, uint32_t out[5])
+{
+  out[0] = b.total[kBatchPrepare];
+  out[1] = b.total[kBatchInterp] + b.total[kBatchInterp3];
+  out[2] = b.total[kBatchGather];
+  out[3] = b.total[kBatchSpread];
+  out[4] = b.total[kBatchFinish];
 }
 }  // namespace
 
@@ -148,6 +191,29 @@ gnufft_status gnufft_batch_create(gnufft_plan *const *plans,
                        n_instances * sizeof(BatchInst),
                        cudaMemcpyHostToDevice));
     b->counters.reset(kBatchStages * sizeof(unsigned));
+    // side streams for the transforms: one per distinct cuFFT plan, at most
+    // kSideStreams
+    b->fft_stream.resize(n_instances);
+    std::vector<cufftHandle> seen;
+    for (uint32_t i = 0; i < n_instances; ++i)
+    {
+      auto it = std::find(seen.begin(), seen.end(), b->fft[i]);
+      const int k = (int)(it - seen.begin());
+      if (it == seen.end())
+        seen.push_back(b->fft[i]);
+      b->fft_stream[i] = k % kSideStreams;
+    }
+    const int ns = std::min<int>(kSideStreams, (int)seen.size());
+    GN_CUDA(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (int k = 0; k < ns; ++k)
+    {
+      cudaStream_t st;
+      GN_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+      b->side.push_back(st);
+      cudaEvent_t e;
+      GN_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      b->join.push_back(e);
+    }
     *out = b.release();
   });
 }
@@ -176,6 +242,9 @@ gnufft_status gnufft_batch_forward(gnufft_batch *b, const void *const *images,
     run_ffts(*b, CUFFT_FORWARD, s);
     launch_batch_stage(kBatchInterp, inst, (int)b->n, b->total[kBatchInterp],
                        &b->io, cnt + kBatchInterp, b->interp_smem, s);
+    launch_batch_stage(kBatchInterp3, inst, (int)b->n,
+                       b->total[kBatchInterp3], &b->io, cnt + kBatchInterp3,
+                       b->interp_smem, s);
   });
 }
 
@@ -216,9 +285,9 @@ gnufft_status gnufft_batch_get_info(const gnufft_batch *b,
   return guarded([&] {
     check_batch(b);
     info->n_instances = b->n;
-    for (int st = 0; st < kBatchStages; ++st)
-      info->units[st] = b->total[st];
-    info->kernels_forward = 2;
+    public_units(*b, info->units);
+    info->kernels_forward = 1 + (b->total[kBatchInterp] > 0) +
+                            (b->total[kBatchInterp3] > 0);
     info->kernels_adjoint = 3;
     info->fft_calls = b->n;
     info->device_bytes =

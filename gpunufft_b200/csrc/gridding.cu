@@ -956,16 +956,20 @@ __device__ __forceinline__ void forward_interp_unit(
           float2 gv[KS];
 #pragma unroll
           for (int x = 0; x < KS; ++x)
-            if (x < nx)
-              gv[x] = tile[(size_t)(rowb + x0 + x) * PITCH + coil];
+          {
+            if (x >= nx)
+              break;
+            gv[x] = tile[(size_t)(rowb + x0 + x) * PITCH + coil];
+          }
 #pragma unroll
           for (int x = 0; x < KS; ++x)
-            if (x < nx)
-            {
-              const float w = __fmul_rn(wzy, wx[x]);
-              ax = __fmaf_rn(gv[x].x, w, ax);
-              ay = __fmaf_rn(gv[x].y, w, ay);
-            }
+          {
+            if (x >= nx)
+              break;
+            const float w = __fmul_rn(wzy, wx[x]);
+            ax = __fmaf_rn(gv[x].x, w, ax);
+            ay = __fmaf_rn(gv[x].y, w, ay);
+          }
         }
       }
       const int t = b0 + i;
@@ -1711,6 +1715,7 @@ int slots_for(const Geo &g) { return g.kw + 1 <= 4 ? 4 : 8; }
 // --------------------------------------------------------------------------
 // batches: one persistent launch per stage over all instances
 // --------------------------------------------------------------------------
+constexpr int kBatchSlots = 8;
 // Copies instance i's descriptor into shared memory (all threads; a
 // barrier follows) unless it is already there.
 __device__ __forceinline__ void batch_load(const BatchInst *__restrict__ inst,
@@ -1804,25 +1809,18 @@ __device__ __forceinline__ void batch_interp_unit(const BatchInst &b,
                                b.fwd_cg);
 }
 
-__global__ void __launch_bounds__(kThreads)
+// One launch per dimensionality (its own unit list); 8 footprint slots
+// (kernel widths up to 7) for every instance, so that each launch holds a
+// single instantiation of the interpolation.
+template <int DIM>
+__global__ void __launch_bounds__(kThreads, 3)
     k_batch_interp(const BatchInst *__restrict__ inst, int n, uint32_t total,
                    unsigned *counter, const __grid_constant__ BatchIo io)
 {
   extern __shared__ float2 smem[];
-  batch_loop(inst, n, kBatchInterp, total, counter,
+  batch_loop(inst, n, DIM == 2 ? kBatchInterp : kBatchInterp3, total, counter,
              [&](int i, uint32_t u, const BatchInst &b) {
-               float2 *out = io.out[i];
-               if (b.g.dim == 3)
-               {
-                 if (b.slots == 4)
-                   batch_interp_unit<3, 4>(b, u, out, smem);
-                 else
-                   batch_interp_unit<3, 8>(b, u, out, smem);
-               }
-               else if (b.slots == 4)
-                 batch_interp_unit<2, 4>(b, u, out, smem);
-               else
-                 batch_interp_unit<2, 8>(b, u, out, smem);
+               batch_interp_unit<DIM, kBatchSlots>(b, u, io.out[i], smem);
              });
 }
 
@@ -2390,16 +2388,16 @@ void batch_configure(BatchInst &b, int tile_coils)
   const Geo &g = b.g;
   b.spmm_cg = spmm_coil_group(b.C);
   b.CP = (b.C + b.spmm_cg - 1) / b.spmm_cg * b.spmm_cg;
-  b.slots = slots_for(g);
+  b.slots = kBatchSlots;
   int cg = forward_coil_group(b.C, g.dim, g.pad);
   if (tile_coils > 0)
     cg = tile_coils > 32 ? 32 : pow2_at_least(tile_coils);
   if (g.dim == 3 && cg > 8)
     cg = 8;
-  // tiles within 72 KB keep three blocks of the interpolation stage per SM
-  while (cg > 1 && forward_smem_bytes(g, cg) > 72 * 1024)
-    cg >>= 1;
   b.fwd_cg = cg;
+  // tiles within 72 KB keep three blocks of the interpolation stage per SM
+  while (b.fwd_cg > 1 && batch_interp_smem(b) > 72 * 1024)
+    b.fwd_cg >>= 1;
   const int X = g.G[0];
   const int work = (X & 1) == 0 ? X / 2 : X;
   b.tpr = work >= 64 ? 64 : (work > 0 ? work : 1);
@@ -2411,8 +2409,10 @@ void batch_units(const BatchInst &b, uint32_t units[kBatchStages])
   const uint32_t rpb = kThreads / b.tpr;
   units[kBatchPrepare] =
       (uint32_t)((g.G[1] + rpb - 1) / rpb) * g.G[2] * (uint32_t)b.C;
-  units[kBatchInterp] =
+  const uint32_t interp =
       (uint32_t)b.n_items * (uint32_t)((b.C + b.fwd_cg - 1) / b.fwd_cg);
+  units[kBatchInterp] = g.dim == 2 ? interp : 0;
+  units[kBatchInterp3] = g.dim == 3 ? interp : 0;
   units[kBatchGather] = (uint32_t)((b.M + kGatherSamples - 1) / kGatherSamples) *
                         (uint32_t)((b.CP + kGatherCoils - 1) / kGatherCoils);
   units[kBatchSpread] =
@@ -2424,7 +2424,12 @@ void batch_units(const BatchInst &b, uint32_t units[kBatchStages])
 
 size_t batch_interp_smem(const BatchInst &b)
 {
-  return forward_smem_bytes(b.g, b.fwd_cg);
+  const Geo &g = b.g;
+  const size_t cells =
+      g.dim == 3 ? (size_t)g.pad * g.pad * g.pad : (size_t)g.pad * g.pad;
+  return cells * (b.fwd_cg + 1) * sizeof(float2) +
+         (size_t)kThreads * (g.dim + g.dim * kBatchSlots) * 4 + 8 +
+         (size_t)g.pad * 16;
 }
 
 namespace
@@ -2459,11 +2464,18 @@ unsigned launch_batch_stage(int stage, const BatchInst *inst, int n,
     k_batch_prepare<<<nb, kThreads, 0, s>>>(inst, n, total, counter, *io);
     break;
   case kBatchInterp:
-    set_smem(k_batch_interp, interp_smem);
+    set_smem(k_batch_interp<2>, interp_smem);
     nb = std::min<unsigned>(total,
-                            resident_blocks(k_batch_interp, interp_smem));
-    k_batch_interp<<<nb, kThreads, interp_smem, s>>>(inst, n, total, counter,
-                                                     *io);
+                            resident_blocks(k_batch_interp<2>, interp_smem));
+    k_batch_interp<2><<<nb, kThreads, interp_smem, s>>>(inst, n, total,
+                                                        counter, *io);
+    break;
+  case kBatchInterp3:
+    set_smem(k_batch_interp<3>, interp_smem);
+    nb = std::min<unsigned>(total,
+                            resident_blocks(k_batch_interp<3>, interp_smem));
+    k_batch_interp<3><<<nb, kThreads, interp_smem, s>>>(inst, n, total,
+                                                        counter, *io);
     break;
   case kBatchGather:
     nb = std::min<unsigned>(total, resident_blocks(k_batch_gather, 0));

@@ -137,7 +137,8 @@ constexpr int kBatchMax = 512;
 enum BatchStage
 {
   kBatchPrepare = 0,  // S x, deapodization, pad, shift (forward)
-  kBatchInterp,       // interpolation to the samples (forward)
+  kBatchInterp,       // interpolation to the samples (forward, 2-D)
+  kBatchInterp3,      // the same for 3-D instances (its own launch)
   kBatchGather,       // k-space to sorted, coil-interleaved order (adjoint)
   kBatchSpread,       // interpolation matrix x k-space into the grid
   kBatchFinish,       // crop, scale, deapodization, conj(S) coil sum
@@ -152,7 +153,7 @@ struct BatchInst
   int CP;       // coil lanes of the sorted k-space (multiple of spmm_cg)
   int spmm_cg;  // coils per spread group
   int fwd_cg;   // coils per forward tile
-  int slots;    // footprint slots per axis (4 or 8)
+  int slots;    // footprint slots per axis of the interpolation stage
   int signs;    // grid cells multiplied by (-1)^(x+y+z) before the forward
                 // transform (grids even along every axis)
   int tpr;      // prepare: threads per grid row

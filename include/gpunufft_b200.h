@@ -309,9 +309,12 @@ GNUFFT_API gnufft_status gnufft_get_stage_times(const gnufft_plan *plan,
  * kernel widths, sector widths and coil counts -- with every gridding
  * stage of all instances in one persistent launch: forward = prepare
  * (maps, deapodization, pad, shift), one cuFFT call per instance,
- * interpolation; adjoint = k-space gather, spread, one cuFFT call per
- * instance, finish (crop, deapodization, conj(maps) coil sum).  Each stage's
- * blocks take (instance, work item) units from a device counter.
+ * interpolation (one launch per dimensionality present); adjoint = k-space
+ * gather, spread, one cuFFT call per instance, finish (crop,
+ * deapodization, conj(maps) coil sum).  Each stage's blocks take
+ * (instance, work item) units from a device counter.  The cuFFT calls run
+ * on up to 8 side streams of the batch, forked from and joined back into
+ * the caller's stream (instances sharing a plan share a side stream).
  *
  * gnufft_batch_create: plans[i] and n_coils[i] describe instance i (n_coils
  * must equal the plan's map channels when it has maps); one plan may appear

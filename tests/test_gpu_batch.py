@@ -103,7 +103,9 @@ def test_persistent_batch_frames_3d_density_texture():
     bo = BatchedOperator(plans, coils)
     info = bo.info()
     assert info.n_instances == 6 and info.fft_calls == 6
-    assert info.kernels_forward == 2 and info.kernels_adjoint == 3
+    # prepare, then one interpolation launch for the 2-D and one for the
+    # 3-D instances
+    assert info.kernels_forward == 3 and info.kernels_adjoint == 3
     assert all(u > 0 for u in info.units) and info.device_bytes > 0
     imgs = [torch.randn(p.img_shape if p.n_sens else (c,) + p.img_shape,
                         dtype=torch.complex64, device="cuda")
