@@ -1412,7 +1412,9 @@ __global__ void __launch_bounds__(kThreads, MINB)
 #pragma unroll
       for (int c = 0; c < CG; ++c)
         acc[c] = make_float2(0.f, 0.f);
-      const int xb = l0[s][0] + dx;
+      // y and x unrolled over the footprint slots with early exits, so that
+      // their weights are register reads (no select over the slots)
+      const int row0 = (l0[s][2] * pad + l0[s][1]) * pad + l0[s][0] + dx;
       for (int z = 0; z < n[s][2]; ++z)
       {
         float wzv = 0.f;
@@ -1420,15 +1422,13 @@ __global__ void __launch_bounds__(kThreads, MINB)
         for (int k = 0; k < KS; ++k)
           if (k == z)
             wzv = w[s][2][k];
-        for (int y = 0; y < n[s][1]; ++y)
-        {
-          float wyv = 0.f;
 #pragma unroll
-          for (int k = 0; k < KS; ++k)
-            if (k == y)
-              wyv = w[s][1][k];
-          const float wzy = __fmul_rn(wzv, wyv);
-          const int row = ((l0[s][2] + z) * pad + l0[s][1] + y) * pad + xb;
+        for (int y = 0; y < KS; ++y)
+        {
+          if (y >= n[s][1])
+            break;
+          const float wzy = __fmul_rn(wzv, w[s][1][y]);
+          const int row = row0 + (z * pad + y) * pad;
 #pragma unroll
           for (int x = 0; x < KS; ++x)
           {
