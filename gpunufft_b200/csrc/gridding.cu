@@ -1291,7 +1291,15 @@ __global__ void __launch_bounds__(kThreads, MINB)
       issue(gi);
   }
 
-  // footprints of this thread's samples (tile frame), kept for all groups
+  // Items of at most kThreads / 2 samples (most of them) run two coil
+  // groups at once: the block's halves take groups g and g + 1 (both tile
+  // buffers), each thread of a half one sample; larger items walk the
+  // groups one at a time.  The copy schedule is the same either way (group
+  // g in buffer g % nbuf, its copy issued once group g - nbuf is done).
+  const int nsamp = it.end - it.begin;
+  const bool two = inside && nbuf == 2 && nsamp <= kThreads / 2;
+  const int half = two ? (int)(threadIdx.x / (kThreads / 2)) : 0;
+  const int first = two ? (int)(threadIdx.x % (kThreads / 2)) : threadIdx.x;
   // footprint, original position and sqrt(density) of this thread's
   // samples (the item's samples in lane order), kept for all coil groups
   int l0[kFwdSpt][3], n[kFwdSpt][3];
@@ -1301,7 +1309,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
 #pragma unroll
   for (int s = 0; s < kFwdSpt; ++s)
   {
-    const int k = it.begin + threadIdx.x + s * kThreads;
+    const int k = it.begin + first + s * kThreads;
     const bool live = k < it.end;
     const uint32_t t = live ? (order ? __ldg(order + k) : (uint32_t)k) : 0u;
     jdst[s] = 0;
@@ -1331,17 +1339,21 @@ __global__ void __launch_bounds__(kThreads, MINB)
     }
   }
 
-  for (int gi = 0; gi < ng; ++gi)
+  const int step = two ? 2 : 1;
+  for (int gi = 0; gi < ng; gi += step)
   {
-    const int buf = inside ? gi % nbuf : 0;
-    const float4 *tile = tiles + (size_t)buf * tstride;
+    const int gn = min(step, ng - gi);  // groups of this phase
+    const int gh = gi + half;           // this half's group
+    const float4 *tile =
+        tiles + (size_t)(inside ? gh % nbuf : 0) * tstride;
     if (inside)
     {
       // the k-th use of a buffer completes phase k of its barrier
-      if (threadIdx.x == 0 &&
-          !mbar_wait_bounded(bar_base + 8u * (uint32_t)buf,
-                             (uint32_t)(gi / nbuf) & 1u, cw.polls))
-        s_fail = 1;
+      if (threadIdx.x == 0)
+        for (int q = gi; q < gi + gn; ++q)
+          if (!mbar_wait_bounded(bar_base + 8u * (uint32_t)(q % nbuf),
+                                 (uint32_t)(q / nbuf) & 1u, cw.polls))
+            s_fail = 1;
       __syncthreads();
       if (s_fail)
       {  // a copy did not complete: report, and give the copies still in
@@ -1391,7 +1403,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
     // performFFTScaling then performDensityCompensation
     // (std_gpuNUFFT_kernels.cu:114-140, 220-242)
     auto emit = [&](int c, float2 a, int s) {
-      const int cc = gi * CG + c;
+      const int cc = gh * CG + c;
       if (cc < C)
       {
         float ax = __fmul_rn(a.x, scale), ay = __fmul_rn(a.y, scale);
@@ -1406,7 +1418,7 @@ __global__ void __launch_bounds__(kThreads, MINB)
 #pragma unroll
     for (int s = 0; s < kFwdSpt; ++s)
     {
-      if (it.begin + threadIdx.x + s * kThreads >= it.end)
+      if (gh >= ng || it.begin + first + s * kThreads >= it.end)
         continue;
       float2 acc[CG];
 #pragma unroll
@@ -1451,9 +1463,11 @@ __global__ void __launch_bounds__(kThreads, MINB)
       for (int c = 0; c < CG; ++c)
         emit(c, acc[c], s);
     }
-    __syncthreads();  // this group's buffer is free
-    if (inside && threadIdx.x == 0 && gi + nbuf < ng)
-      issue(gi + nbuf);
+    __syncthreads();  // this phase's buffers are free
+    if (inside && threadIdx.x == 0)
+      for (int q = gi; q < gi + gn; ++q)
+        if (q + nbuf < ng)
+          issue(q + nbuf);
   }
 }
 
