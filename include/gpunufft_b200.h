@@ -319,8 +319,10 @@ GNUFFT_API gnufft_status gnufft_get_stage_times(const gnufft_plan *plan,
  * gnufft_batch_create: plans[i] and n_coils[i] describe instance i (n_coils
  * must equal the plan's map channels when it has maps); one plan may appear
  * several times (frames sharing a trajectory).  All plans on one device;
- * they must outlive the batch, and their maps must not be replaced with a
- * different channel count while it exists.  The batch owns the instances'
+ * they must outlive the batch, and their maps must not be removed or
+ * replaced with a different channel count while it exists (the batch reads
+ * the plans' tables and maps in place; maps replaced with the same channel
+ * count are read in their new values).  The batch owns the instances'
  * scratch (grid and sorted k-space).  At most 512 instances.
  *
  * gnufft_batch_forward: images[i] (device): [n_coils][image] complex64, or
