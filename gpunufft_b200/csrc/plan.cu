@@ -358,12 +358,19 @@ void set_sens_host(gnufft_plan &p, const void *sens, uint32_t n_coils)
   }
   const size_t n = (size_t)n_coils * p.g.img_count;
   const float2 *s = static_cast<const float2 *>(sens);
-  p.sens_h.assign(s, s + n);
+  // only the plain flow (maps copied per coil per call, like the upstream)
+  // needs a host copy; the other plans copy from the caller's buffer (the
+  // callers synchronise the plan's stream before they return)
+  if (p.plain)
+    p.sens_h.assign(s, s + n);
+  else
+    p.sens_h.clear();
   // keep the device buffer when it is large enough (no free / malloc, which
   // would synchronise the device, when maps are swapped between requests)
   p.sens.ensure(n * sizeof(float2));
-  GN_CUDA(cudaMemcpyAsync(p.sens.get(), p.sens_h.data(), n * sizeof(float2),
-                          cudaMemcpyHostToDevice, p.stream));
+  GN_CUDA(cudaMemcpyAsync(p.sens.get(), p.plain ? p.sens_h.data() : s,
+                          n * sizeof(float2), cudaMemcpyHostToDevice,
+                          p.stream));
   p.sens_coils = n_coils;
 }
 
