@@ -81,8 +81,8 @@ struct gnufft_plan
   cudaTextureObject_t lut_tex = 0;
 
   // host copies of the exported tables
-  std::vector<float> lut_h, traj_sorted_h, dens_sorted_h, deapo_h;
-  std::vector<uint32_t> di_h, sdc_h, centers_h, order_h;
+  std::vector<float> lut_h, deapo_h;
+  std::vector<uint32_t> sdc_h, centers_h, order_h;
   bool has_dens = false;
 
   // resident device tables
@@ -466,10 +466,6 @@ void create_plan(gnufft_plan &p, const gnufft_desc *d, const float *traj,
   histogram_offsets(p.sec_sorted.as<uint32_t>(), M, (uint32_t)p.g.n_sectors,
                     sdc.as<uint32_t>(), s);
   download(p.sdc_h, sdc, (size_t)p.g.n_sectors + 1, s);
-  download(p.di_h, p.di, M, s);
-  download(p.traj_sorted_h, p.traj_sorted, (size_t)dim * M, s);
-  if (dens)
-    download(p.dens_sorted_h, p.dens_sorted, M, s);
   GN_CUDA(cudaStreamSynchronize(s));
   set_sens_host(p, sens, sens ? d->n_coils : 0);
   finish_tables(p);
@@ -525,8 +521,6 @@ void load_plan(gnufft_plan &p, const gnufft_desc *d, const float *traj_sorted,
       ss[t] = sct;
     }
   p.sdc_h.assign(sdc, sdc + S + 1);
-  p.di_h.assign(di, di + M);
-  p.traj_sorted_h.assign(traj_sorted, traj_sorted + (size_t)dim * M);
   p.deapo_h.assign(deapo, deapo + p.g.img_count);
   cudaStream_t s = p.stream;
   upload(p.di, di, M, s);
@@ -535,7 +529,6 @@ void load_plan(gnufft_plan &p, const gnufft_desc *d, const float *traj_sorted,
   if (dens_sorted)
   {
     p.has_dens = true;
-    p.dens_sorted_h.assign(dens_sorted, dens_sorted + M);
     upload(p.dens_sorted, dens_sorted, M, s);
   }
   set_sens_host(p, sens, sens ? d->n_coils : 0);
@@ -1143,13 +1136,20 @@ gnufft_status gnufft_export_tables(const gnufft_plan *p, float *traj_sorted,
       if (dst && !v.empty())
         std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
     };
-    cp(traj_sorted, p->traj_sorted_h);
-    cp(data_indices, p->di_h);
+    // the per-sample tables are read from the device (complete since the
+    // plan's creation synchronised its stream)
+    DeviceGuard dg(p->desc.device);
+    auto dl = [](void *dst, const DeviceBuffer &b, size_t bytes) {
+      if (dst && bytes)
+        GN_CUDA(cudaMemcpy(dst, b.get(), bytes, cudaMemcpyDeviceToHost));
+    };
+    dl(traj_sorted, p->traj_sorted, (size_t)p->dim * p->M * sizeof(float));
+    dl(data_indices, p->di, (size_t)p->M * sizeof(uint32_t));
     cp(sector_data_count, p->sdc_h);
     cp(processing_order, p->order_h);
     cp(sector_centers, p->centers_h);
     if (p->has_dens)
-      cp(dens_sorted, p->dens_sorted_h);
+      dl(dens_sorted, p->dens_sorted, (size_t)p->M * sizeof(float));
     cp(deapo, p->deapo_h);
     cp(kernel_lut, p->lut_h);
   });
