@@ -9,7 +9,7 @@
 // takes whole rows and runs the inverse x transform in place before writing
 // only the cropped outputs (k_adjoint_spmm_xfft).
 //
-// Forward: one block per work item (<= 512 samples of one sector) stages the
+// Forward: one block per work item (<= 256 samples of one sector) stages the
 // sector tile plus halo of a coil group in shared memory -- by tensor copies
 // when the grid holds the FORWARD-shifted spectrum and the tile is a box of
 // it, else by cp.async gathers with wrap-around and shift folded in -- and

@@ -14,7 +14,7 @@ namespace gnufft
 
 // Forward work item: samples [begin, end) of one sector, at most
 // kFwdItemSamples of them.
-constexpr int kFwdItemSamples = 512;
+constexpr int kFwdItemSamples = 256;
 struct FwdItem
 {
   int sector;
