@@ -1200,7 +1200,8 @@ __global__ void __launch_bounds__(kThreads)
 // The same interpolation with every coil group of an item in one block (3-D
 // grids written with coil pairs interleaved, cell q of coil c at
 // ((c / 2) * G + q) * 2 + c % 2).  Each thread computes the footprint of
-// its (at most two) samples once, in registers; the samples of an item are
+// its samples (kFwdSpt per thread: one for items of up to 256 samples)
+// once, in registers; the samples of an item are
 // taken in the plan's lane order (build_forward_lane_order), which puts
 // samples whose footprints start in different shared-memory bank groups on
 // each eight adjacent lanes, so that the 16-byte tile reads of a quarter
