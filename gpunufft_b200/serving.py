@@ -21,6 +21,7 @@ from __future__ import annotations
 import collections
 import dataclasses
 import hashlib
+import os
 import time
 from typing import Deque, Dict, List, Optional, Sequence, Tuple
 
@@ -121,11 +122,22 @@ class PlanCache:
     instances of one trajectory's operator exist (two: a second request of
     the same trajectory runs beside the first); a request whose
     trajectory's instances are all busy waits for one.  Idle instances stay
-    cached until memory is needed."""
+    cached until memory is needed.
 
-    def __init__(self, device: int = 0, max_instances: int = 2):
+    With ``plan_dir`` the operators' precomputed tables also persist on
+    disk, one ``<key>.npz`` per trajectory (``Plan.save``: the upstream's
+    precompute arrays): a miss loads the file when it exists (tables
+    validated, ``Plan.from_file``; the sort is skipped) and otherwise
+    creates the operator and writes its file, so a restarted server meets
+    known trajectories with their tables ready."""
+
+    def __init__(self, device: int = 0, max_instances: int = 2,
+                 plan_dir: Optional[str] = None):
         self.device = device
         self.max_instances = max_instances
+        self.plan_dir = plan_dir
+        self.plans_loaded = 0
+        self.plans_saved = 0
         self.free: Dict[str, List[Plan]] = collections.defaultdict(list)
         self.busy: Dict[int, str] = {}
         self.count: Dict[str, int] = collections.defaultdict(int)
@@ -152,11 +164,25 @@ class PlanCache:
             p = self.free[key].pop()
         else:
             self.misses += 1
-            p = Plan(req.traj, req.img_dims, req.kernel_width,
-                     req.sector_width, req.osf, req.dens, None, C.BALANCED,
-                     device=self.device)
+            p = self._new_plan(req, key)
             self.count[key] += 1
         self.busy[id(p)] = key
+        return p
+
+    def _new_plan(self, req: Request, key: str) -> Plan:
+        path = (os.path.join(self.plan_dir, key + ".npz")
+                if self.plan_dir else None)
+        if path and os.path.exists(path):
+            self.plans_loaded += 1
+            return Plan.from_file(path, device=self.device)
+        p = Plan(req.traj, req.img_dims, req.kernel_width, req.sector_width,
+                 req.osf, req.dens, None, C.BALANCED, device=self.device)
+        if path:
+            os.makedirs(self.plan_dir, exist_ok=True)
+            tmp = os.path.join(self.plan_dir, key + ".tmp.npz")
+            p.save(tmp)
+            os.replace(tmp, path)  # readers never see a partial file
+            self.plans_saved += 1
         return p
 
     def release(self, p: Plan) -> None:
@@ -272,14 +298,15 @@ class Server:
     90 % of the free memory at start)."""
 
     def __init__(self, device: int = 0, max_slots: int = 8,
-                 memory_budget: Optional[int] = None):
+                 memory_budget: Optional[int] = None,
+                 plan_dir: Optional[str] = None):
         self.device = device
         torch.cuda.set_device(device)
         free, _ = torch.cuda.mem_get_info(device)
         self.budget = int(memory_budget if memory_budget is not None
                           else 0.9 * free)
         self.max_slots = max_slots
-        self.cache = PlanCache(device)
+        self.cache = PlanCache(device, plan_dir=plan_dir)
         self.queue: Deque[Request] = collections.deque()
         self.active: List[_Active] = []
         self.done: List[Request] = []
@@ -412,6 +439,8 @@ class Server:
             "peak_admitted_gb": self.peak_accounted / 1e9,
             "plan_cache_hits": self.cache.hits,
             "plan_cache_misses": self.cache.misses,
+            "plans_loaded": self.cache.plans_loaded,
+            "plans_saved": self.cache.plans_saved,
         }
 
     def close(self) -> None:

@@ -112,3 +112,29 @@ def test_operator_resident_per_trajectory():
     finally:
         s.close()
     assert st["plan_cache_misses"] == 1 and st["plan_cache_hits"] == 1
+
+
+def test_operators_persist_on_disk(tmp_path):
+    """A server with a plan directory writes one plan file per trajectory;
+    a second server (fresh cache, same directory) loads them instead of
+    sorting again, and gives the same results."""
+    from gpunufft_b200.serving import Server
+    reqs = _requests()[:4]  # four distinct trajectories, 2-D and 3-D
+    first = Server(max_slots=2, plan_dir=str(tmp_path))
+    try:
+        done1 = {r.rid: r.result for r in first.run(reqs)}
+        st1 = first.stats()
+    finally:
+        first.close()
+    assert st1["plans_saved"] == 4 and st1["plans_loaded"] == 0
+    assert len(list(tmp_path.glob("*.npz"))) == 4
+    again = _requests()[:4]
+    second = Server(max_slots=2, plan_dir=str(tmp_path))
+    try:
+        done2 = {r.rid: r.result for r in second.run(again)}
+        st2 = second.stats()
+    finally:
+        second.close()
+    assert st2["plans_loaded"] == 4 and st2["plans_saved"] == 0
+    for rid, x in done1.items():
+        assert rel_l2(done2[rid], x) < TOL, rid
