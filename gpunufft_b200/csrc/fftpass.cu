@@ -182,22 +182,27 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
   }
 }
 
-// Tile t of a pass over `planes` planes of n_ct column tiles.  PAIRED:
-// the two planes (coils) of a pair take adjacent tiles (t, t + 1 ->
-// planes 2p, 2p + 1 of the same columns, so that the two halves of every
-// interleaved output pair are written close in time); an odd last plane
-// follows on its own.
-// PAIRED: a tile holds TC / 2 columns of both planes (coils) of a pair,
-// copied as two boxes into two planes of L rows; output element (plane c,
+// Tile t of a pass over `planes` planes of n_ct column tiles (PAIRED 0:
+// plane t / n_ct, columns (t % n_ct) * TC ...).  PAIRED > 0: a tile holds
+// TC / 2 columns of both planes (coils) of a pair; output element (plane c,
 // row r, column col) goes to ((c / 2) * dst_rows * ncols + r * ncols + col)
 // * 2 + c % 2, i.e. coil pairs interleaved (the layout the 3-D forward
 // interpolation reads two coils of a cell from with one 16-byte load), and
 // every warp store covers TC / 2 whole pairs.  Tile t: pair t / n_ct,
-// column tile t % n_ct (n_ct counted in TC / 2 columns); the second plane of
-// an odd last pair is an out-of-range box (zero fill).
-template <int L, bool INV, bool PAIRED>
+// column tile t % n_ct (n_ct counted in TC / 2 columns).  Tile layouts in
+// shared memory: PAIRED 0, rows of TC columns of one plane; PAIRED 1, the
+// two coils as two planes of L rows x TC / 2 columns (two 3-D boxes; the
+// second plane of an odd last pair is an out-of-range box, zero fill; the
+// two planes' rows share banks); PAIRED 2, one 4-D box (columns, coil in
+// pair, rows, pair) that interleaves the coils' half rows, so that tile row
+// r holds TC / 2 columns of the first coil, then of the second -- the
+// layout of PAIRED 0, read without bank conflicts.  `tail` (PAIRED 2)
+// covers an odd last coil (pair tail_pl) with a one-coil map whose second
+// coil is out of range (zero fill).
+template <int L, bool INV, int PAIRED>
 __global__ void __launch_bounds__(Shape<L>::CT, 3)
     k_fft_cols_tma(const __grid_constant__ CUtensorMap tmap,
+                   const __grid_constant__ CUtensorMap tail, long long tail_pl,
                    float2 *__restrict__ dst, long long ncols, long long n_ct,
                    long long n_tiles, int box_rows, int ncopy, int dst_rows,
                    int in_add, int in_count, int out_add, int out_count,
@@ -221,7 +226,15 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
     const long long pl = t / n_ct, ct = t - pl * n_ct;
     const uint32_t dst = buf0 + (uint32_t)b * (uint32_t)T::tile_bytes;
     const uint32_t bar = bar0 + 8u * (uint32_t)b;
-    if (PAIRED)
+    if (PAIRED == 2)
+    {  // both coils of pair pl, half rows interleaved
+      tma::mbar_expect_tx(bar, bytes);
+      if (pl == tail_pl)
+        tma::copy_4d(dst, &tail, (int)ct * CW, 0, 0, 0, bar);
+      else
+        tma::copy_4d(dst, &tmap, (int)ct * CW, 0, 0, (int)pl, bar);
+    }
+    else if (PAIRED == 1)
     {  // both planes of pair pl, each into its own L rows
       tma::mbar_expect_tx(bar, bytes);  // two boxes of half the columns
       tma::copy_3d(dst, &tmap, (int)ct * CW, 0, (int)(2 * pl), bar);
@@ -278,8 +291,8 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
       cr = __ldg(colrange + col);
     const bool on = col < ncols && cr.x <= cr.y;
     float2 bv[S::R2];
-    col_tile_fft<L, INV, PAIRED>(buf + (size_t)b * L * TC, cl, lt, in_add,
-                                 in_count, w, tw, bv);
+    col_tile_fft<L, INV, PAIRED == 1>(buf + (size_t)b * L * TC, cl, lt,
+                                      in_add, in_count, w, tw, bv);
     if (lt < S::R1 && on)
     {
       const long long psz = (long long)dst_rows * ncols;
@@ -406,6 +419,195 @@ __global__ void __launch_bounds__(Shape<L>::CT, L <= 256 ? 3 : 1)
       }
       out[px] = r;
     }
+  }
+}
+
+// The same pass with the coil combine (stage 2, maps) on tensor-copy
+// tiles.  A persistent block walks its units (unit u: TC adjacent columns
+// (u / groups) * TC ..., coil group u % groups) and in each unit its coils
+// in order.  Per coil, two copies bring the column tile (L rows x TC
+// columns) and the coil-map tile (n_out rows x TC columns) into one of two
+// stages, so that the copies of the next coil (or of the next unit's first
+// coil) are in flight while the current one is transformed in place (as in
+// k_fft_cols_tma).  Deapodization is read once per unit.  Arithmetic and
+// coil order are those of k_fft_cols_sum, so both give the same results.
+template <int L> struct SumTma
+{
+  using S = Shape<L>;
+  static constexpr uint32_t src_bytes = (uint32_t)(L * S::TC * sizeof(float2));
+  __host__ __device__ static uint32_t sens_bytes(int n_out)
+  {
+    return (uint32_t)(n_out * S::TC * sizeof(float2));
+  }
+  static size_t smem(int n_out)
+  {
+    return 2 * ((size_t)src_bytes + sens_bytes(n_out)) +
+           (size_t)L * sizeof(float2) + 2 * 8 + 16;
+  }
+};
+
+template <int L>
+__global__ void __launch_bounds__(Shape<L>::CT, 2)
+    k_fft_cols_sum_tma(const __grid_constant__ CUtensorMap src_map,
+                       const __grid_constant__ CUtensorMap sens_map,
+                       long long ncols, long long n_units, int groups,
+                       int cpb, int C, const float *__restrict__ deapo,
+                       int n_out, long long N, int out_add, float scale,
+                       int accumulate, const float2 *__restrict__ roots,
+                       float2 *__restrict__ out, float2 *__restrict__ partial,
+                       tma::CopyWait cw)
+{
+  using S = Shape<L>;
+  using T = SumTma<L>;
+  constexpr int TC = S::TC;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float2 *src_t = reinterpret_cast<float2 *>(smraw);  // 2 x L x TC
+  float2 *sens_t = src_t + 2 * L * TC;                 // 2 x n_out x TC
+  float2 *tw = sens_t + 2 * (size_t)n_out * TC;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(tw + L);
+  int &s_fail = *reinterpret_cast<int *>(mbar + 2);
+  const uint32_t bar0 = tma::smem_addr(mbar);
+  const uint32_t src0 = tma::smem_addr(src_t);
+  const uint32_t sens0 = tma::smem_addr(sens_t);
+  const uint32_t sens_bytes = T::sens_bytes(n_out);
+  // job cursor: unit u, coil c of the unit's coils [c0, c1)
+  struct Cur
+  {
+    long long u;
+    int c, c1;
+  };
+  auto start = [&](long long u) {
+    Cur k;
+    k.u = u;
+    k.c = (int)(u % groups) * cpb;
+    k.c1 = min(C, k.c + cpb);
+    return k;
+  };
+  auto next = [&](Cur k) {
+    if (++k.c >= k.c1)
+      k = start(k.u + gridDim.x);
+    return k;
+  };
+  auto issue = [&](const Cur &k, int b) {
+    const uint32_t bar = bar0 + 8u * (uint32_t)b;
+    const int col0 = (int)((k.u / groups) * TC);
+    tma::mbar_expect_tx(bar, T::src_bytes + sens_bytes);
+    tma::copy_3d(src0 + (uint32_t)b * T::src_bytes, &src_map, col0, 0, k.c,
+                 bar);
+    tma::copy_3d(sens0 + (uint32_t)b * sens_bytes, &sens_map, col0, 0, k.c,
+                 bar);
+  };
+  Cur ic = start(blockIdx.x);  // the next job to copy (uniform)
+  if (threadIdx.x == 0)
+  {
+    s_fail = 0;
+    tma::mbar_init(bar0);
+    tma::mbar_init(bar0 + 8u);
+    tma::mbar_init_fence();
+    if (ic.u < n_units)
+      issue(ic, 0);
+  }
+  ic = next(ic);
+  if (threadIdx.x == 0 && ic.u < n_units)
+    issue(ic, 1);
+  ic = next(ic);
+  load_roots(tw, roots, L);
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  const int cl = threadIdx.x % TC, lt = threadIdx.x / TC;
+  float2 acc[S::R2];
+  float d[S::R2];
+  long long i = 0;
+  for (Cur cc = start(blockIdx.x); cc.u < n_units; ++i)
+  {
+    const int b = (int)(i & 1);
+    if (threadIdx.x == 0 &&
+        !tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b,
+                                (uint32_t)(i >> 1) & 1u, cw.polls))
+      s_fail = 1;
+    __syncthreads();
+    const Cur nx = next(cc);
+    if (s_fail)
+    {  // a copy did not complete: report it and give the copies in flight
+       // (this job's, the next one's) a bounded wait before returning
+      if (threadIdx.x == 0)
+      {
+        atomicExch(cw.err, 1);
+        tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b,
+                               (uint32_t)(i >> 1) & 1u);
+        if (nx.u < n_units)
+          tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)(b ^ 1),
+                                 (uint32_t)((i + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    const long long col = (cc.u / groups) * TC + cl;
+    const bool on = col < ncols && lt < S::R1;
+    if (cc.c == (int)(cc.u % groups) * cpb)
+    {  // the unit's first coil: its deapodization, a zero sum
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int n = (lt + S::R1 * k2 + out_add) & (L - 1);
+        d[k2] = (on && n < n_out) ? __ldg(deapo + (long long)n * ncols + col)
+                                  : 0.f;
+        acc[k2] = make_float2(0.f, 0.f);
+      }
+    }
+    float2 bv[S::R2];
+    col_tile_fft<L, true, false>(src_t + (size_t)b * L * TC, cl, lt, 0, L, w,
+                                 tw, bv);
+    if (on)
+    {
+      const float2 *st = sens_t + (size_t)b * n_out * TC;
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int n = (lt + S::R1 * k2 + out_add) & (L - 1);
+        if (n >= n_out)
+          continue;
+        // crop -> FFT scaling -> deapodization -> conj(S) * v, running coil
+        // sum (gpuNUFFT_operator.cpp:800-819, std_gpuNUFFT_kernels.cu:
+        // 158-218)
+        float2 v = make_float2(__fmul_rn(bv[k2].x, scale),
+                               __fmul_rn(bv[k2].y, scale));
+        v.x = __fmul_rn(v.x, d[k2]);
+        v.y = __fmul_rn(v.y, d[k2]);
+        const float2 sv = st[n * TC + cl];
+        acc[k2].x += v.x * sv.x + v.y * sv.y;
+        acc[k2].y += v.y * sv.x - v.x * sv.y;
+      }
+    }
+    tma::fence_proxy_async();  // the in-place writes before the refill
+    __syncthreads();           // stage b is free
+    if (threadIdx.x == 0 && ic.u < n_units)
+      issue(ic, b);
+    ic = next(ic);
+    if (nx.u != cc.u && on)
+    {  // the unit's last coil: its sum (or the group's partial sum)
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+      {
+        const int n = (lt + S::R1 * k2 + out_add) & (L - 1);
+        if (n >= n_out)
+          continue;
+        const long long px = (long long)n * ncols + col;
+        if (partial)
+        {
+          partial[(cc.u % groups) * N + px] = acc[k2];
+          continue;
+        }
+        float2 r = acc[k2];
+        if (accumulate)
+        {
+          const float2 o = out[px];
+          r = make_float2(o.x + r.x, o.y + r.y);
+        }
+        out[px] = r;
+      }
+    }
+    cc = nx;
   }
 }
 
@@ -728,6 +930,55 @@ bool col_tensor_map(CUtensorMap &tm, const float2 *base, long long ncols,
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+// Tensor maps of the coil-pair tiles with interleaved half rows: 4-D
+// (columns, coil in pair, rows, pair), box CW columns x 2 coils x box_rows
+// rows x 1 pair, so that the box lands in shared memory as rows of CW
+// columns of the first coil followed by CW of the second.  `tm` covers the
+// planes / 2 whole pairs; with an odd plane count, `tail` covers the last
+// plane as a pair whose second coil is out of range (zero fill).  False
+// when TMA is unavailable or rejects the layout.
+bool col_pair_tensor_maps(CUtensorMap &tm, CUtensorMap &tail,
+                          const float2 *base, long long ncols, int rows,
+                          long long plane_stride, long long planes, int CW,
+                          int box_rows)
+{
+  tma::EncodeTiledFn enc = tma::encode_fn();
+  if (!enc || (ncols & 1) || (plane_stride & 1) ||
+      (reinterpret_cast<uintptr_t>(base) & 15))
+    return false;
+  auto make = [&](CUtensorMap &m, const float2 *b, long long coils,
+                  long long pairs) {
+    cuuint64_t dims[4] = {(cuuint64_t)ncols, (cuuint64_t)coils,
+                          (cuuint64_t)rows, (cuuint64_t)pairs};
+    cuuint64_t strides[3] = {(cuuint64_t)plane_stride * sizeof(float2),
+                             (cuuint64_t)ncols * sizeof(float2),
+                             (cuuint64_t)(2 * plane_stride) * sizeof(float2)};
+    cuuint32_t box[4] = {(cuuint32_t)CW, 2, (cuuint32_t)box_rows, 1};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(&m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4,
+               const_cast<float2 *>(b), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  const long long pairs = planes / 2;
+  if (planes & 1)
+  {
+    if (!make(tail, base + (planes - 1) * plane_stride, 1, 1))
+      return false;
+    if (pairs == 0)
+    {
+      tm = tail;
+      return true;
+    }
+  }
+  if (!make(tm, base, 2, pairs))
+    return false;
+  if (!(planes & 1))
+    tail = tm;
+  return true;
+}
+
 // Persistent blocks of the tensor-copy passes: three per SM.
 unsigned persistent_blocks(long long work)
 {
@@ -758,23 +1009,44 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
         const int cw = paired ? S::TC / 2 : S::TC;
         if (paired && ncopy != 1)
           return;
-        CUtensorMap tm;
-        if (!col_tensor_map(tm, src, ncols, src_rows,
-                            (long long)src_rows * ncols, planes, cw,
-                            box_rows))
-          return;
+        CUtensorMap tm, tail;
+        long long tail_pl = -1;
+        // paired: interleaved half rows (one 4-D box) where the tensor
+        // maps take that layout, else two planes
+        int mode = 0;
+        if (paired &&
+            col_pair_tensor_maps(tm, tail, src, ncols, src_rows,
+                                 (long long)src_rows * ncols, planes, cw,
+                                 box_rows))
+        {
+          mode = 2;
+          if (planes & 1)
+            tail_pl = planes / 2;
+        }
+        else
+        {
+          if (!col_tensor_map(tm, src, ncols, src_rows,
+                              (long long)src_rows * ncols, planes, cw,
+                              box_rows))
+            return;
+          tail = tm;
+          mode = paired ? 1 : 0;
+        }
         const long long n_ct = (ncols + cw - 1) / cw;
         const long long n_tiles = n_ct * (paired ? (planes + 1) / 2 : planes);
         auto launch = [&](auto k) {
           set_smem(k, ColTma<LL>::smem());
           k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
-              tm, dst, ncols, n_ct, n_tiles, box_rows, ncopy, dst_rows,
-              in_add, in_count, out_add, out_count, roots, colrange, wait);
+              tm, tail, tail_pl, dst, ncols, n_ct, n_tiles, box_rows, ncopy,
+              dst_rows, in_add, in_count, out_add, out_count, roots, colrange,
+              wait);
         };
-        if (paired)
-          launch(k_fft_cols_tma<LL, INV, true>);
+        if (mode == 2)
+          launch(k_fft_cols_tma<LL, INV, 2>);
+        else if (mode == 1)
+          launch(k_fft_cols_tma<LL, INV, 1>);
         else
-          launch(k_fft_cols_tma<LL, INV, false>);
+          launch(k_fft_cols_tma<LL, INV, 0>);
         GN_LAUNCH_CHECK("pruned column transform (tensor-copy tiles)");
         done = true;
       }
@@ -797,6 +1069,45 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
                                           out_count, roots, colrange);
     GN_LAUNCH_CHECK("pruned column transform");
   });
+}
+
+// The coil-combining last adjoint pass on tensor-copy tiles, where it
+// applies: lengths up to 256, two blocks per SM, layouts the tensor maps
+// take.  False (nothing launched) otherwise.
+template <int L>
+bool launch_cols_sum_tma(const float2 *src, long long ncols,
+                         long long coil_stride, const float *deapo,
+                         const float2 *sens, int n_out, long long N, int C,
+                         int groups, int cpb, int out_add, float scale,
+                         int accumulate, const float2 *roots, float2 *out,
+                         float2 *partial, tma::CopyWait cw, cudaStream_t s)
+{
+  if constexpr (L > 256)
+    return false;
+  else
+  {
+    using S = Shape<L>;
+    const size_t smem = SumTma<L>::smem(n_out);
+    if (!cw.err || smem > 113 * 1024 || n_out > L || (N & 1))
+      return false;
+    CUtensorMap src_map, sens_map;
+    if (!col_tensor_map(src_map, src, ncols, L, coil_stride, C, S::TC, L) ||
+        !col_tensor_map(sens_map, sens, ncols, n_out, N, C, S::TC, n_out))
+      return false;
+    const long long nb = (ncols + S::TC - 1) / S::TC;
+    const long long n_units = nb * groups;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long blocks = n_units < 2LL * sms ? n_units : 2LL * sms;
+    auto k = k_fft_cols_sum_tma<L>;
+    set_smem(k, smem);
+    k<<<(unsigned)blocks, S::CT, smem, s>>>(
+        src_map, sens_map, ncols, n_units, groups, cpb, C, deapo, n_out, N,
+        out_add, scale, accumulate, roots, out, partial, cw);
+    GN_LAUNCH_CHECK("pruned adjoint last pass (tensor-copy tiles)");
+    return true;
+  }
 }
 
 }  // namespace
@@ -978,7 +1289,12 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
     const bool combine = sens != nullptr && stage == 2;
     float2 *partial = (combine && groups > 1) ? part : nullptr;
     const dim3 grd((unsigned)nb, (unsigned)groups);
-    if (combine)
+    const bool tiles =
+        combine && launch_cols_sum_tma<LL>(src, ncols, coil_stride, deapo,
+                                           sens, g.N[ax], N, C, groups, cpb,
+                                           out_add, g.fft_scale, accumulate,
+                                           roots[ax], out, partial, cw, s);
+    if (combine && !tiles)
     {
       auto k = k_fft_cols_sum<LL, true>;
       set_smem(k, S::col_smem());
@@ -987,7 +1303,7 @@ void launch_pruned_adjoint_xfirst(const float2 *xrows, const float *deapo,
                                          g.fft_scale, stage, accumulate,
                                          roots[ax], out, partial);
     }
-    else
+    else if (!combine)
     {
       auto k = k_fft_cols_sum<LL, false>;
       set_smem(k, S::col_smem());
