@@ -703,6 +703,162 @@ __global__ void __launch_bounds__(kFftThreads, L <= 256 ? 4 : 1)
   }
 }
 
+// The same pass on tensor-copy tiles (at least NL coils, N_x <= 256, N_x a
+// multiple of 4): a persistent block walks its jobs (job j: image row
+// j / n_cc, coils (j % n_cc) * NL ..., one line per coil) through two
+// stages.  Per job one tensor copy brings the NL coil rows (the maps with
+// SENS, else the per-coil images; coils past C are out of range, zero
+// fill) and untiled copies bring the image row (SENS) and the
+// deapodization row, so that the copies of the job after next are in
+// flight while the current one is transformed: a stage is refilled as soon
+// as the first DFT stage, its only reader, is done.  Arithmetic is that of
+// k_fft_rows_fwd, so both give the same results.
+struct RowsTma
+{
+  static __host__ __device__ uint32_t up128(uint32_t v)
+  {
+    return (v + 127u) & ~127u;
+  }
+  // per stage: coil rows, image row, deapodization row
+  static __host__ __device__ uint32_t coil_bytes(int NL, int Nx)
+  {
+    return up128((uint32_t)(NL * Nx * 8));
+  }
+  static __host__ __device__ uint32_t img_bytes(int Nx)
+  {
+    return up128((uint32_t)(Nx * 8));
+  }
+  static __host__ __device__ uint32_t stage_bytes(int NL, int Nx)
+  {
+    return coil_bytes(NL, Nx) + img_bytes(Nx) + up128((uint32_t)(Nx * 4));
+  }
+};
+
+template <int L, bool SENS>
+__global__ void __launch_bounds__(kFftThreads, 3)
+    k_fft_rows_fwd_tma(const __grid_constant__ CUtensorMap coil_map,
+                       const float2 *__restrict__ image,
+                       const float *__restrict__ deapo, int Nx,
+                       long long rows, int C, long long n_jobs, int n_cc,
+                       int in_add, int out_add,
+                       const float2 *__restrict__ roots,
+                       float2 *__restrict__ A, tma::CopyWait cw)
+{
+  using S = Shape<L>;
+  constexpr int NL = S::NL;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  const uint32_t cb = RowsTma::coil_bytes(NL, Nx);
+  const uint32_t ib = RowsTma::img_bytes(Nx);
+  const uint32_t sb = RowsTma::stage_bytes(NL, Nx);
+  float2 *tw = reinterpret_cast<float2 *>(smraw + 2 * sb);
+  float2 *Ybase = tw + L;
+  uint64_t *mbar = reinterpret_cast<uint64_t *>(Ybase + NL * S::R1 * S::YP);
+  int &s_fail = *reinterpret_cast<int *>(mbar + 2);
+  const uint32_t bar0 = tma::smem_addr(mbar);
+  const uint32_t st0 = tma::smem_addr(smraw);
+  const uint32_t tx = (uint32_t)(NL * Nx * 8) + (SENS ? (uint32_t)(Nx * 8) : 0u) +
+                      (uint32_t)(Nx * 4);
+  const long long stride = gridDim.x;
+  auto issue = [&](long long j, int b) {
+    const long long r = j / n_cc;
+    const int c0 = (int)(j - r * n_cc) * NL;
+    const uint32_t dst = st0 + (uint32_t)b * sb;
+    const uint32_t bar = bar0 + 8u * (uint32_t)b;
+    tma::mbar_expect_tx(bar, tx);
+    tma::copy_2d(dst, &coil_map, (int)(r * Nx), c0, bar);
+    if (SENS)
+      tma::copy_bulk(dst + cb, image + r * Nx, (uint32_t)(Nx * 8), bar);
+    tma::copy_bulk(dst + cb + ib, deapo + r * Nx, (uint32_t)(Nx * 4), bar);
+  };
+  if (threadIdx.x == 0)
+  {
+    s_fail = 0;
+    tma::mbar_init(bar0);
+    tma::mbar_init(bar0 + 8u);
+    tma::mbar_init_fence();
+    if (blockIdx.x < n_jobs)
+      issue(blockIdx.x, 0);
+    if (blockIdx.x + stride < n_jobs)
+      issue(blockIdx.x + stride, 1);
+  }
+  load_roots(tw, roots, L);
+  __syncthreads();
+  float2 w[Rm<L>::V / 2];
+  load_reg_roots<L>(w, tw);
+  const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
+  float2 *Y = Ybase + line * S::R1 * S::YP;
+  int i = 0;
+  for (long long j = blockIdx.x; j < n_jobs; j += stride, ++i)
+  {
+    const int b = i & 1;
+    if (threadIdx.x == 0 &&
+        !tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b,
+                                (uint32_t)(i >> 1) & 1u, cw.polls))
+      s_fail = 1;
+    __syncthreads();  // also: the previous job's exchange reads are done
+    if (s_fail)
+    {  // a copy did not complete: report it and give the copies in flight
+       // (this job's, the next one's) a bounded wait before returning
+      if (threadIdx.x == 0)
+      {
+        atomicExch(cw.err, 1);
+        tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)b,
+                               (uint32_t)(i >> 1) & 1u);
+        if (j + stride < n_jobs)
+          tma::mbar_wait_bounded(bar0 + 8u * (uint32_t)(b ^ 1),
+                                 (uint32_t)((i + 1) >> 1) & 1u);
+      }
+      return;
+    }
+    const long long row = j / n_cc;
+    const int c = (int)(j - row * n_cc) * NL + line;
+    const unsigned char *stg = smraw + (size_t)b * sb;
+    const float2 *crow = reinterpret_cast<const float2 *>(stg) + line * Nx;
+    const float2 *img = reinterpret_cast<const float2 *>(stg + cb);
+    const float *dea = reinterpret_cast<const float *>(stg + cb + ib);
+    if (lt < S::R2)
+    {
+      // FFT input n = lt + R2 j holds image x (n + in_add) mod L when < Nx
+      float2 a[S::R1];
+#pragma unroll
+      for (int q = 0; q < S::R1; ++q)
+      {
+        const int xp = (lt + S::R2 * q + in_add) & (L - 1);
+        float2 v = make_float2(0.f, 0.f);
+        if (xp < Nx)
+        {
+          if (SENS)
+          {  // sensMulKernel, then deapodization (std_gpuNUFFT_kernels.cu)
+            const float2 x = img[xp];
+            const float2 sv = crow[xp];
+            v.x = x.x * sv.x - x.y * sv.y;
+            v.y = x.x * sv.y + x.y * sv.x;
+          }
+          else
+            v = crow[xp];
+          const float d = dea[xp];
+          v.x = __fmul_rn(v.x, d);
+          v.y = __fmul_rn(v.y, d);
+        }
+        a[q] = v;
+      }
+      stage1<L, false, 1>(a, lt, w, tw, Y);
+    }
+    __syncthreads();  // stage b read; exchange written
+    if (threadIdx.x == 0 && j + 2 * stride < n_jobs)
+      issue(j + 2 * stride, b);
+    if (lt < S::R1 && c < C)
+    {
+      float2 bv[S::R2];
+      stage2<L, false, 1>(bv, lt, w, Y);
+      float2 *out = A + ((long long)c * rows + row) * L;
+#pragma unroll
+      for (int k2 = 0; k2 < S::R2; ++k2)
+        out[(lt + S::R1 * k2 + out_add) & (L - 1)] = bv[k2];
+    }
+  }
+}
+
 // --------------------------------------------------------------------------
 // adjoint rows: inverse DFT along x, crop + shift, scale, deapodization,
 // conj(sens) coil sum
@@ -1110,6 +1266,71 @@ bool launch_cols_sum_tma(const float2 *src, long long ncols,
   }
 }
 
+// The forward row pass on tensor-copy tiles, where it applies (see
+// k_fft_rows_fwd_tma); false (nothing launched) otherwise.
+template <int L>
+bool launch_rows_fwd_tma(const float2 *image, const float2 *sens,
+                         const float *deapo, int Nx, long long rows,
+                         long long N, int C, int in_add, int out_add,
+                         const float2 *roots, float2 *A, tma::CopyWait cw,
+                         cudaStream_t s)
+{
+  if constexpr (L > 256)
+    return false;
+  else
+  {
+    using S = Shape<L>;
+    constexpr int NL = S::NL;
+    const float2 *coils = sens ? sens : image;
+    tma::EncodeTiledFn enc = tma::encode_fn();
+    if (!enc || !cw.err || C < NL || Nx > 256 || Nx > L || (Nx & 3) ||
+        (reinterpret_cast<uintptr_t>(image) & 15) ||
+        (reinterpret_cast<uintptr_t>(coils) & 15) ||
+        (reinterpret_cast<uintptr_t>(deapo) & 15))
+      return false;
+    const size_t smem = 2 * (size_t)RowsTma::stage_bytes(NL, Nx) +
+                        (size_t)L * sizeof(float2) +
+                        (size_t)NL * S::R1 * S::YP * sizeof(float2) + 2 * 8 +
+                        16;
+    if (smem > 113 * 1024)
+      return false;
+    // coil rows: (pixel, coil), box N_x pixels x NL coils
+    CUtensorMap tm;
+    cuuint64_t dims[2] = {(cuuint64_t)N, (cuuint64_t)C};
+    cuuint64_t strides[1] = {(cuuint64_t)N * sizeof(float2)};
+    cuuint32_t box[2] = {(cuuint32_t)Nx, (cuuint32_t)NL};
+    cuuint32_t estr[2] = {1, 1};
+    if (enc(&tm, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2,
+            const_cast<float2 *>(coils), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    const int n_cc = (C + NL - 1) / NL;
+    const long long n_jobs = rows * n_cc;
+    auto launch = [&](auto k) {
+      set_smem(k, smem);
+      int dev = 0, sms = 148, per_sm = 1;
+      if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+              &per_sm, k, kFftThreads, smem) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+      const long long cap = (long long)per_sm * sms;
+      k<<<(unsigned)(n_jobs < cap ? n_jobs : cap), kFftThreads, smem, s>>>(
+          tm, image, deapo, Nx, rows, C, n_jobs, n_cc, in_add, out_add, roots,
+          A, cw);
+    };
+    if (sens)
+      launch(k_fft_rows_fwd_tma<L, true>);
+    else
+      launch(k_fft_rows_fwd_tma<L, false>);
+    GN_LAUNCH_CHECK("pruned forward rows (tensor-copy tiles)");
+    return true;
+  }
+}
+
 }  // namespace
 
 bool pruned_fft_supported(const Geo &g)
@@ -1161,6 +1382,9 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
     const int in_add = pos_mod((long long)g.shift_inv[0] - g.crop[0], g.G[0]);
     // the FORWARD fftshift: frequency k is stored at (k - ceil(G/2)) mod G
     const int out_add = pos_mod(-(long long)g.shift_fwd[0], g.G[0]);
+    if (launch_rows_fwd_tma<LL>(image, sens, deapo, g.N[0], rows, N, C,
+                                in_add, out_add, roots[0], tmp_a, cw, s))
+      return;
     if (sens)
     {
       auto k = k_fft_rows_fwd<LL, true>;

@@ -105,6 +105,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar,
 // Bulk tensor copies global -> shared, completion counted on `bar`.  The
 // innermost coordinate times the element size must be a multiple of 16
 // bytes (callers start tiles on such columns).
+__device__ __forceinline__ void copy_2d(uint32_t dst, const void *tmap,
+                                        int x, int y, uint32_t bar)
+{
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::"
+      "complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
 __device__ __forceinline__ void copy_3d(uint32_t dst, const void *tmap,
                                         int x, int y, int z, uint32_t bar)
 {
@@ -125,6 +135,18 @@ __device__ __forceinline__ void copy_4d(uint32_t dst, const void *tmap,
       "complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
       "l"(reinterpret_cast<uint64_t>(tmap)), "r"(x), "r"(y), "r"(z), "r"(w),
       "r"(bar)
+      : "memory");
+}
+
+// Untiled bulk copy global -> shared of `bytes` bytes (both addresses
+// 16-byte aligned, bytes a multiple of 16), completion counted on `bar`.
+__device__ __forceinline__ void copy_bulk(uint32_t dst, const void *src,
+                                          uint32_t bytes, uint32_t bar)
+{
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes "
+      "[%0], [%1], %2, [%3];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(bar)
       : "memory");
 }
 
