@@ -41,6 +41,29 @@ template <int L> struct Shape
   }
 };
 
+// Division of integers 0 <= n < 2^31 by a fixed divisor d >= 1 with one
+// wide multiply and a shift: q = (n * m) >> p, m = ceil(2^p / d),
+// p = 31 + ceil(log2 d) (the round-up method of Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994; exact
+// because (m d - 2^p) n < d 2^31 <= 2^p).
+struct FastDiv
+{
+  uint32_t d = 1, m = 1u << 31, p = 31;
+  FastDiv() = default;
+  __host__ explicit FastDiv(uint32_t div) : d(div)
+  {
+    uint32_t l = 0;
+    while ((1ull << l) < div)
+      ++l;
+    p = 31 + l;
+    m = (uint32_t)(((1ull << p) + div - 1) / div);
+  }
+  __host__ __device__ uint32_t div(uint32_t n) const
+  {
+    return (uint32_t)(((uint64_t)n * m) >> p);
+  }
+};
+
 __host__ __device__ constexpr int bitrev(int i, int R)
 {
   int r = 0;

@@ -203,8 +203,8 @@ template <int L, bool INV, int PAIRED>
 __global__ void __launch_bounds__(Shape<L>::CT, 3)
     k_fft_cols_tma(const __grid_constant__ CUtensorMap tmap,
                    const __grid_constant__ CUtensorMap tail, long long tail_pl,
-                   float2 *__restrict__ dst, long long ncols, long long n_ct,
-                   long long n_tiles, int box_rows, int ncopy, int dst_rows,
+                   float2 *__restrict__ dst, long long ncols, FastDiv n_ct,
+                   int n_tiles, int box_rows, int ncopy, int dst_rows,
                    int in_add, int in_count, int out_add, int out_count,
                    const float2 *__restrict__ roots,
                    const uint2 *__restrict__ colrange, tma::CopyWait cw)
@@ -220,10 +220,10 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
   const uint32_t bar0 = tma::smem_addr(mbar);
   const uint32_t buf0 = tma::smem_addr(buf);
   const uint32_t bytes = (uint32_t)(ncopy * box_rows) * 128u;
-  const long long stride = gridDim.x;
+  const int stride = gridDim.x;
   constexpr int CW = PAIRED ? TC / 2 : TC;  // columns per tile
-  auto issue = [&](long long t, int b) {
-    const long long pl = t / n_ct, ct = t - pl * n_ct;
+  auto issue = [&](int t, int b) {
+    const int pl = (int)n_ct.div((uint32_t)t), ct = t - pl * (int)n_ct.d;
     const uint32_t dst = buf0 + (uint32_t)b * (uint32_t)T::tile_bytes;
     const uint32_t bar = bar0 + 8u * (uint32_t)b;
     if (PAIRED == 2)
@@ -262,7 +262,7 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
   load_reg_roots<L>(w, tw);
   const int cl = threadIdx.x % TC, lt = threadIdx.x / TC;
   int i = 0;
-  for (long long t = blockIdx.x; t < n_tiles; t += stride, ++i)
+  for (int t = blockIdx.x; t < n_tiles; t += stride, ++i)
   {
     const int b = i & 1;
     if (threadIdx.x == 0 &&
@@ -283,9 +283,9 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
       }
       return;
     }
-    const long long pl = t / n_ct, ct = t - pl * n_ct;
-    const long long plane = PAIRED ? 2 * pl + cl / CW : pl;
-    const long long col = ct * CW + cl % CW;
+    const int pl = (int)n_ct.div((uint32_t)t), ct = t - pl * (int)n_ct.d;
+    const long long plane = PAIRED ? 2LL * pl + cl / CW : pl;
+    const long long col = (long long)ct * CW + cl % CW;
     uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
     if (colrange && col < ncols)
       cr = __ldg(colrange + col);
@@ -450,7 +450,7 @@ template <int L>
 __global__ void __launch_bounds__(Shape<L>::CT, 2)
     k_fft_cols_sum_tma(const __grid_constant__ CUtensorMap src_map,
                        const __grid_constant__ CUtensorMap sens_map,
-                       long long ncols, long long n_units, int groups,
+                       long long ncols, int n_units, FastDiv groups,
                        int cpb, int C, const float *__restrict__ deapo,
                        int n_out, long long N, int out_add, float scale,
                        int accumulate, const float2 *__restrict__ roots,
@@ -473,13 +473,15 @@ __global__ void __launch_bounds__(Shape<L>::CT, 2)
   // job cursor: unit u, coil c of the unit's coils [c0, c1)
   struct Cur
   {
-    long long u;
-    int c, c1;
+    int u, ct, g;  // unit, its column tile and coil group
+    int c, c1;     // coil, end of the group's coils
   };
-  auto start = [&](long long u) {
+  auto start = [&](int u) {
     Cur k;
     k.u = u;
-    k.c = (int)(u % groups) * cpb;
+    k.ct = (int)groups.div((uint32_t)u);
+    k.g = u - k.ct * (int)groups.d;
+    k.c = k.g * cpb;
     k.c1 = min(C, k.c + cpb);
     return k;
   };
@@ -490,7 +492,7 @@ __global__ void __launch_bounds__(Shape<L>::CT, 2)
   };
   auto issue = [&](const Cur &k, int b) {
     const uint32_t bar = bar0 + 8u * (uint32_t)b;
-    const int col0 = (int)((k.u / groups) * TC);
+    const int col0 = k.ct * TC;
     tma::mbar_expect_tx(bar, T::src_bytes + sens_bytes);
     tma::copy_3d(src0 + (uint32_t)b * T::src_bytes, &src_map, col0, 0, k.c,
                  bar);
@@ -542,9 +544,9 @@ __global__ void __launch_bounds__(Shape<L>::CT, 2)
       }
       return;
     }
-    const long long col = (cc.u / groups) * TC + cl;
+    const long long col = (long long)cc.ct * TC + cl;
     const bool on = col < ncols && lt < S::R1;
-    if (cc.c == (int)(cc.u % groups) * cpb)
+    if (cc.c == cc.g * cpb)
     {  // the unit's first coil: its deapodization, a zero sum
 #pragma unroll
       for (int k2 = 0; k2 < S::R2; ++k2)
@@ -595,7 +597,7 @@ __global__ void __launch_bounds__(Shape<L>::CT, 2)
         const long long px = (long long)n * ncols + col;
         if (partial)
         {
-          partial[(cc.u % groups) * N + px] = acc[k2];
+          partial[cc.g * N + px] = acc[k2];
           continue;
         }
         float2 r = acc[k2];
@@ -739,7 +741,7 @@ __global__ void __launch_bounds__(kFftThreads, 3)
     k_fft_rows_fwd_tma(const __grid_constant__ CUtensorMap coil_map,
                        const float2 *__restrict__ image,
                        const float *__restrict__ deapo, int Nx,
-                       long long rows, int C, long long n_jobs, int n_cc,
+                       long long rows, int C, int n_jobs, FastDiv n_cc,
                        int in_add, int out_add,
                        const float2 *__restrict__ roots,
                        float2 *__restrict__ A, tma::CopyWait cw)
@@ -758,10 +760,10 @@ __global__ void __launch_bounds__(kFftThreads, 3)
   const uint32_t st0 = tma::smem_addr(smraw);
   const uint32_t tx = (uint32_t)(NL * Nx * 8) + (SENS ? (uint32_t)(Nx * 8) : 0u) +
                       (uint32_t)(Nx * 4);
-  const long long stride = gridDim.x;
-  auto issue = [&](long long j, int b) {
-    const long long r = j / n_cc;
-    const int c0 = (int)(j - r * n_cc) * NL;
+  const int stride = gridDim.x;
+  auto issue = [&](int j, int b) {
+    const long long r = n_cc.div((uint32_t)j);
+    const int c0 = (j - (int)r * (int)n_cc.d) * NL;
     const uint32_t dst = st0 + (uint32_t)b * sb;
     const uint32_t bar = bar0 + 8u * (uint32_t)b;
     tma::mbar_expect_tx(bar, tx);
@@ -788,7 +790,7 @@ __global__ void __launch_bounds__(kFftThreads, 3)
   const int line = threadIdx.x / S::T, lt = threadIdx.x % S::T;
   float2 *Y = Ybase + line * S::R1 * S::YP;
   int i = 0;
-  for (long long j = blockIdx.x; j < n_jobs; j += stride, ++i)
+  for (int j = blockIdx.x; j < n_jobs; j += stride, ++i)
   {
     const int b = i & 1;
     if (threadIdx.x == 0 &&
@@ -810,8 +812,8 @@ __global__ void __launch_bounds__(kFftThreads, 3)
       }
       return;
     }
-    const long long row = j / n_cc;
-    const int c = (int)(j - row * n_cc) * NL + line;
+    const long long row = n_cc.div((uint32_t)j);
+    const int c = (j - (int)row * (int)n_cc.d) * NL + line;
     const unsigned char *stg = smraw + (size_t)b * sb;
     const float2 *crow = reinterpret_cast<const float2 *>(stg) + line * Nx;
     const float2 *img = reinterpret_cast<const float2 *>(stg + cb);
@@ -1190,10 +1192,13 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
         }
         const long long n_ct = (ncols + cw - 1) / cw;
         const long long n_tiles = n_ct * (paired ? (planes + 1) / 2 : planes);
+        if (n_tiles >= (1LL << 31) - 2LL * persistent_blocks(n_tiles))
+          return;  // tile indices are 31-bit
         auto launch = [&](auto k) {
           set_smem(k, ColTma<LL>::smem());
           k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
-              tm, tail, tail_pl, dst, ncols, n_ct, n_tiles, box_rows, ncopy,
+              tm, tail, tail_pl, dst, ncols, FastDiv((uint32_t)n_ct),
+              (int)n_tiles, box_rows, ncopy,
               dst_rows, in_add, in_count, out_add, out_count, roots, colrange,
               wait);
         };
@@ -1252,6 +1257,8 @@ bool launch_cols_sum_tma(const float2 *src, long long ncols,
       return false;
     const long long nb = (ncols + S::TC - 1) / S::TC;
     const long long n_units = nb * groups;
+    if (n_units >= (1LL << 30))
+      return false;  // unit indices are 31-bit
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess)
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1259,7 +1266,8 @@ bool launch_cols_sum_tma(const float2 *src, long long ncols,
     auto k = k_fft_cols_sum_tma<L>;
     set_smem(k, smem);
     k<<<(unsigned)blocks, S::CT, smem, s>>>(
-        src_map, sens_map, ncols, n_units, groups, cpb, C, deapo, n_out, N,
+        src_map, sens_map, ncols, (int)n_units, FastDiv((uint32_t)groups),
+        cpb, C, deapo, n_out, N,
         out_add, scale, accumulate, roots, out, partial, cw);
     GN_LAUNCH_CHECK("pruned adjoint last pass (tensor-copy tiles)");
     return true;
@@ -1308,6 +1316,8 @@ bool launch_rows_fwd_tma(const float2 *image, const float2 *sens,
       return false;
     const int n_cc = (C + NL - 1) / NL;
     const long long n_jobs = rows * n_cc;
+    if (n_jobs >= (1LL << 30))
+      return false;  // job indices are 31-bit
     auto launch = [&](auto k) {
       set_smem(k, smem);
       int dev = 0, sms = 148, per_sm = 1;
@@ -1319,8 +1329,8 @@ bool launch_rows_fwd_tma(const float2 *image, const float2 *sens,
         per_sm = 1;
       const long long cap = (long long)per_sm * sms;
       k<<<(unsigned)(n_jobs < cap ? n_jobs : cap), kFftThreads, smem, s>>>(
-          tm, image, deapo, Nx, rows, C, n_jobs, n_cc, in_add, out_add, roots,
-          A, cw);
+          tm, image, deapo, Nx, rows, C, (int)n_jobs, FastDiv((uint32_t)n_cc),
+          in_add, out_add, roots, A, cw);
     };
     if (sens)
       launch(k_fft_rows_fwd_tma<L, true>);
