@@ -80,6 +80,30 @@ __device__ __forceinline__ float2 cmul(float2 a, float2 b)
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+// Two-lane FP32 add / subtract (one sm_100 paired instruction; each lane
+// rounds to nearest like the scalar operation, so results are identical).
+__device__ __forceinline__ float2 add2(float2 a, float2 b)
+{
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+  float2 r;
+  asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
+      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
+      "sub.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
+
 __host__ __device__ constexpr int ilog2(int v)
 {
   int r = 0;
@@ -123,16 +147,21 @@ __device__ __forceinline__ void reg_fft(float2 (&a)[R],
       if (2 * k == half)
       {  // the quarter-turn root -i (+i inverse): exact, no multiply
         v = INV ? make_float2(-v.y, v.x) : make_float2(v.y, -v.x);
+        a[i0] = make_float2(u.x + v.x, u.y + v.y);
+        a[i1] = make_float2(u.x - v.x, u.y - v.y);
       }
-      else if (k != 0)
+      else
       {
-        float2 r = w[k * (RM >> (st + 1))];
-        if (INV)
-          r.y = -r.y;
-        v = cmul(v, r);
+        if (k != 0)
+        {
+          float2 r = w[k * (RM >> (st + 1))];
+          if (INV)
+            r.y = -r.y;
+          v = cmul(v, r);
+        }
+        a[i0] = add2(u, v);
+        a[i1] = sub2(u, v);
       }
-      a[i0] = make_float2(u.x + v.x, u.y + v.y);
-      a[i1] = make_float2(u.x - v.x, u.y - v.y);
     }
   }
 }
