@@ -3,6 +3,7 @@
 // an order) and integer-exact.
 #include "binning.cuh"
 
+#include <algorithm>
 #include <vector>
 
 #include "footprint.cuh"
@@ -429,16 +430,37 @@ __global__ void k_col_ranges(const uint32_t *__restrict__ row_off, int G0,
 }  // namespace
 
 void build_column_ranges(const uint32_t *row_off, const Geo &g,
-                         DeviceBuffer &range, cudaStream_t s)
+                         DeviceBuffer &range, DeviceBuffer &tiles,
+                         int &n_tiles, cudaStream_t s)
 {
   const size_t cols = (size_t)g.G[0] * g.G[1];
   range.reset(cols * sizeof(uint2));
-  std::vector<uint2> init(cols, make_uint2(0xFFFFFFFFu, 0u));
-  GN_CUDA(cudaMemcpyAsync(range.get(), init.data(), cols * sizeof(uint2),
+  std::vector<uint2> h(cols, make_uint2(0xFFFFFFFFu, 0u));
+  GN_CUDA(cudaMemcpyAsync(range.get(), h.data(), cols * sizeof(uint2),
                           cudaMemcpyHostToDevice, s));
   k_col_ranges<<<grid_for(g.grid_count, 256, 148 * 64), 256, 0, s>>>(
       row_off, g.G[0], g.G[1], g.G[2], range.as<uint2>());
   GN_LAUNCH_CHECK("column ranges");
+  GN_CUDA(cudaMemcpyAsync(h.data(), range.get(), cols * sizeof(uint2),
+                          cudaMemcpyDeviceToHost, s));
+  GN_CUDA(cudaStreamSynchronize(s));
+  // tiles of kColTile adjacent columns with at least one range
+  std::vector<uint32_t> list;
+  const size_t nt = (cols + kColTile - 1) / kColTile;
+  for (size_t t = 0; t < nt; ++t)
+  {
+    bool any = false;
+    for (size_t c = t * kColTile; c < std::min(cols, (t + 1) * kColTile); ++c)
+      any = any || h[c].x <= h[c].y;
+    if (any)
+      list.push_back((uint32_t)t);
+  }
+  n_tiles = (int)list.size();
+  tiles.reset(std::max<size_t>(list.size(), 1) * sizeof(uint32_t));
+  if (!list.empty())
+    GN_CUDA(cudaMemcpyAsync(tiles.get(), list.data(),
+                            list.size() * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice, s));
   GN_CUDA(cudaStreamSynchronize(s));
 }
 

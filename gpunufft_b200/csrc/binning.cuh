@@ -53,7 +53,12 @@ size_t build_interp_matrix(const float *traj_sorted,
 // Per (y, x) column of the grid, the range [lo, hi] of z cells that carry
 // interpolation weights (widened by one; lo > hi when none): the forward
 // transform writes only these cells, the only ones the interpolation reads.
+// `tiles` lists (ascending, n_tiles of them) the tiles of kColTile adjacent
+// columns (tile t: columns t * kColTile ...) that hold at least one range;
+// the forward z pass transforms only those.
+constexpr int kColTile = 8;
 void build_column_ranges(const uint32_t *row_off, const Geo &g,
-                         DeviceBuffer &range, cudaStream_t s);
+                         DeviceBuffer &range, DeviceBuffer &tiles,
+                         int &n_tiles, cudaStream_t s);
 
 }  // namespace gnufft

@@ -207,7 +207,8 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
                    int n_tiles, int box_rows, int ncopy, int dst_rows,
                    int in_add, int in_count, int out_add, int out_count,
                    const float2 *__restrict__ roots,
-                   const uint2 *__restrict__ colrange, tma::CopyWait cw)
+                   const uint2 *__restrict__ colrange,
+                   const uint32_t *__restrict__ tiles, tma::CopyWait cw)
 {
   using S = Shape<L>;
   using T = ColTma<L>;
@@ -222,8 +223,15 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
   const uint32_t bytes = (uint32_t)(ncopy * box_rows) * 128u;
   const int stride = gridDim.x;
   constexpr int CW = PAIRED ? TC / 2 : TC;  // columns per tile
+  auto tile = [&](int t, int &pl, int &ct) {
+    pl = (int)n_ct.div((uint32_t)t);
+    ct = t - pl * (int)n_ct.d;
+    if (tiles)
+      ct = (int)__ldg(tiles + ct);
+  };
   auto issue = [&](int t, int b) {
-    const int pl = (int)n_ct.div((uint32_t)t), ct = t - pl * (int)n_ct.d;
+    int pl, ct;
+    tile(t, pl, ct);
     const uint32_t dst = buf0 + (uint32_t)b * (uint32_t)T::tile_bytes;
     const uint32_t bar = bar0 + 8u * (uint32_t)b;
     if (PAIRED == 2)
@@ -283,7 +291,8 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
       }
       return;
     }
-    const int pl = (int)n_ct.div((uint32_t)t), ct = t - pl * (int)n_ct.d;
+    int pl, ct;
+    tile(t, pl, ct);
     const long long plane = PAIRED ? 2LL * pl + cl / CW : pl;
     const long long col = (long long)ct * CW + cl % CW;
     uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
@@ -1152,7 +1161,9 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
           int src_rows, int dst_rows, long long planes, int in_add,
           int in_count, int out_add, int out_count, const float2 *roots,
           cudaStream_t s, const uint2 *colrange = nullptr,
-          tma::CopyWait wait = tma::CopyWait(), bool paired = false)
+          tma::CopyWait wait = tma::CopyWait(), bool paired = false,
+          const uint32_t *tiles = nullptr, long long n_list = 0,
+          int list_cols = 0)
 {
   bool done = false;
   if (wait.err && L <= 256)
@@ -1190,7 +1201,14 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
           tail = tm;
           mode = paired ? 1 : 0;
         }
-        const long long n_ct = (ncols + cw - 1) / cw;
+        // a list of the column tiles to transform (paired, same width)
+        const bool listed = paired && tiles && list_cols == cw;
+        const long long n_ct = listed ? n_list : (ncols + cw - 1) / cw;
+        if (n_ct == 0)
+        {
+          done = true;  // no column carries a range: nothing to write
+          return;
+        }
         const long long n_tiles = n_ct * (paired ? (planes + 1) / 2 : planes);
         if (n_tiles >= (1LL << 31) - 2LL * persistent_blocks(n_tiles))
           return;  // tile indices are 31-bit
@@ -1200,7 +1218,7 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
               tm, tail, tail_pl, dst, ncols, FastDiv((uint32_t)n_ct),
               (int)n_tiles, box_rows, ncopy,
               dst_rows, in_add, in_count, out_add, out_count, roots, colrange,
-              wait);
+              listed ? tiles : nullptr, wait);
         };
         if (mode == 2)
           launch(k_fft_cols_tma<LL, INV, 2>);
@@ -1380,7 +1398,8 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
                            const uint2 *zrange, tma::CopyWait cw,
-                           bool paired)
+                           bool paired, const uint32_t *ztiles, int n_ztiles,
+                           int ztile_cols)
 {
   const long long N = g.img_count;
   const long long rows = (long long)g.N[1] * g.N[2];
@@ -1425,7 +1444,8 @@ void launch_pruned_forward(const float2 *image, const float2 *sens,
                 g.G[2], C,
                 pos_mod((long long)g.shift_inv[2] - g.crop[2], g.G[2]),
                 g.N[2], pos_mod(-(long long)g.shift_fwd[2], g.G[2]), g.G[2],
-                roots[2], s, zrange, cw, paired);
+                roots[2], s, zrange, cw, paired, ztiles, n_ztiles,
+                ztile_cols);
 }
 
 void launch_pruned_adjoint(const float2 *grid, const float *deapo,

@@ -51,14 +51,18 @@ size_t pruned_scratch_b(const Geo &g, int C);
 // passes load their tiles with plain loads.  paired (3-D, needs err and
 // every grid axis <= 256): the grid is written with coil pairs interleaved,
 // cell q of coil c at ((c / 2) * G + q) * 2 + c % 2 (C rounded up to even
-// coils of storage).
+// coils of storage).  ztiles (paired only): the n_ztiles column tiles of
+// ztile_cols columns (ascending) that hold a z range; the z pass transforms
+// only these (the others have no cell the interpolation reads).
 void launch_pruned_forward(const float2 *image, const float2 *sens,
                            const float *deapo, const Geo &g, int C,
                            const float2 *const roots[3], float2 *tmp_a,
                            float2 *tmp_b, float2 *grid, cudaStream_t s,
                            const uint2 *zrange = nullptr,
                            tma::CopyWait cw = tma::CopyWait(),
-                           bool paired = false);
+                           bool paired = false,
+                           const uint32_t *ztiles = nullptr, int n_ztiles = 0,
+                           int ztile_cols = 0);
 
 // Adjoint: grid [C][G] (INVERSE fftshift folded in by the adjoint spread)
 // -> unnormalised inverse DFT -> crop of the second INVERSE fftshift ->

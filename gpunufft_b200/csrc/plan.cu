@@ -93,6 +93,8 @@ struct gnufft_plan
   DeviceBuffer dlut;          // kernel derivative table (trajectory gradient)
   DeviceBuffer roots[3];      // DFT roots per axis (pruned transforms)
   DeviceBuffer zrange;        // per (y, x) column: z rows with weights
+  DeviceBuffer ztiles;        // column tiles holding a z range
+  int n_ztiles = 0;
   float dlut_mult = 0.f;
   size_t nnz = 0;
   int n_fwd_items = 0;
@@ -144,7 +146,8 @@ struct gnufft_plan
                                   &ks,          &grid,        &stage_in,
                                   &stage_out,   &one_sens,    &fft_a,
                                   &fft_b,       &dlut,        &roots[0],
-                                  &roots[1],    &roots[2],    &zrange};
+                                  &roots[1],    &roots[2],    &zrange,
+                                  &ztiles};
     size_t s = 0;
     for (auto *b : bufs)
       s += b->bytes();
@@ -393,7 +396,8 @@ void finish_tables(gnufft_plan &p)
   launch_invert_permutation(p.di.as<uint32_t>(), p.M, p.di_inv.as<uint32_t>(),
                             p.stream);
   if (p.pruned && p.dim == 3)
-    build_column_ranges(p.w_rows.as<uint32_t>(), p.g, p.zrange, p.stream);
+    build_column_ranges(p.w_rows.as<uint32_t>(), p.g, p.zrange, p.ztiles,
+                        p.n_ztiles, p.stream);
   processing_order(p.sdc_h, p.order_h);
   upload(p.deapo, p.deapo_h.data(), p.deapo_h.size(), p.stream);
   GN_CUDA(cudaStreamSynchronize(p.stream));
@@ -716,7 +720,8 @@ void forward_batched(gnufft_plan &p, const float2 *img, float2 *k, uint32_t C,
     launch_pruned_forward(img, sens, p.deapo.as<float>(), g, (int)C,
                           root_ptrs(p).data(), p.fft_a.as<float2>(),
                           p.fft_b.as<float2>(), grid, s,
-                          p.zrange.as<uint2>(), copy_wait(p), paired);
+                          p.zrange.as<uint2>(), copy_wait(p), paired,
+                          p.ztiles.as<uint32_t>(), p.n_ztiles, kColTile);
     p.launches += g.dim;
     p.mark(5, s);
     p.mark(2, s);

@@ -72,8 +72,9 @@ def plan_table_bytes(req: Request) -> int:
     trajectory before any call: sorted trajectory, indices (sorted order,
     sector, inverse), density weights, the interpolation matrix (row offsets
     per grid cell, at most (kw + 1)^d entries of 8 bytes per sample), the
-    forward work items, their lane order (3-D) and column ranges,
-    deapodization, the lookup table and the maps the request sets."""
+    forward work items, their lane order (3-D), column ranges and the list
+    of column tiles holding one, deapodization, the lookup table and the
+    maps the request sets."""
     dims = [v for v in req.img_dims if v]
     dim = len(dims)
     M = req.traj.shape[1]
@@ -87,7 +88,8 @@ def plan_table_bytes(req: Request) -> int:
         b += 4 * M
     b += 16 * (M // 256 + int(np.prod([-(-g // req.sector_width)
                                        for g in grid])) + 1)
-    b += 8 * grid[0] * grid[1] + 4 * N + 4 * 4096 + 8 * Cn * N
+    b += 8 * grid[0] * grid[1] + 4 * (grid[0] * grid[1] // 8 + 1)
+    b += 4 * N + 4 * 4096 + 8 * Cn * N
     return int(b)
 
 
