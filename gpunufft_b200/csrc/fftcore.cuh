@@ -9,6 +9,8 @@
 
 #include <cuda_runtime.h>
 
+#include "f32x2.cuh"
+
 namespace gnufft
 {
 namespace fftcore
@@ -78,30 +80,6 @@ __host__ __device__ constexpr int bitrev(int i, int R)
 __device__ __forceinline__ float2 cmul(float2 a, float2 b)
 {
   return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-
-// Two-lane FP32 add / subtract (one sm_100 paired instruction; each lane
-// rounds to nearest like the scalar operation, so results are identical).
-__device__ __forceinline__ float2 add2(float2 a, float2 b)
-{
-  float2 r;
-  asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
-      "add.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
-
-__device__ __forceinline__ float2 sub2(float2 a, float2 b)
-{
-  float2 r;
-  asm("{\n\t.reg .b64 pa, pb, pd;\n\t"
-      "mov.b64 pa, {%2, %3};\n\tmov.b64 pb, {%4, %5};\n\t"
-      "sub.rn.f32x2 pd, pa, pb;\n\tmov.b64 {%0, %1}, pd;\n\t}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
 }
 
 __host__ __device__ constexpr int ilog2(int v)
