@@ -12,12 +12,17 @@ import numpy as np
 import pytest
 
 from oracle import nufft_oracle as O
-from tests.helpers import cplx, kooshball_3d, rel_l2
+from tests.helpers import cplx, gaussian_maps, kooshball_3d, rel_l2
 
 pytestmark = pytest.mark.gpu
 
 
-def test_copy_wait_failure_is_reported_and_recoverable():
+@pytest.mark.parametrize("C,maps", [(3, False), (32, True)])
+def test_copy_wait_failure_is_reported_and_recoverable(C, maps):
+    """(3, no maps): the column passes and the forward interpolation wait.
+    (32, maps): the forward's first pass is the persistent row pass (jobs of
+    one image row x 32 coils at this length) and the adjoint's last the
+    persistent coil-sum pass, each with its own bounded waits."""
     torch = pytest.importorskip("torch")
     import gpunufft_b200 as G
     from gpunufft_b200 import _capi
@@ -25,10 +30,10 @@ def test_copy_wait_failure_is_reported_and_recoverable():
     rng = np.random.default_rng(4)
     dims = (16, 16, 16)  # grid 32^3: separable transforms, tensor copies
     traj = kooshball_3d(200, 32)
-    C = 3
-    p = G.Plan(traj, dims, 3, 8, 2.0, None, None, G.BALANCED)
-    ref = O.OracleOperator(traj, dims, 3, 8, 2.0)
-    x = cplx(rng, C, 16, 16, 16)
+    sens = gaussian_maps(C, dims[::-1], rng) if maps else None
+    p = G.Plan(traj, dims, 3, 8, 2.0, None, sens, G.BALANCED)
+    ref = O.OracleOperator(traj, dims, 3, 8, 2.0, None, sens)
+    x = cplx(rng, 16, 16, 16) if maps else cplx(rng, C, 16, 16, 16)
     k = cplx(rng, C, traj.shape[1])
     try:
         assert L.gnufft_set_copy_wait(p._h, 0) == _capi.SUCCESS
