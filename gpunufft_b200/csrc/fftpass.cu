@@ -182,6 +182,66 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
   }
 }
 
+// The same transform for two adjacent columns 2 cp, 2 cp + 1 of a tile of
+// TC-column rows (one 16-byte shared access per row and stage for both,
+// one twiddle load for both).  Outputs k = lt + R1 * k2 in b0 / b1.
+template <int L, bool INV>
+__device__ __forceinline__ void col_tile_fft2(float2 *B, int cp, int lt,
+                                              int in_add, int in_count,
+                                              const float2 (&w)[Rm<L>::V / 2],
+                                              const float2 *tw,
+                                              float2 (&b0)[Shape<L>::R2],
+                                              float2 (&b1)[Shape<L>::R2])
+{
+  using S = Shape<L>;
+  constexpr int TP = S::TC / 2;  // column pairs per tile row
+  float4 *B4 = reinterpret_cast<float4 *>(B);
+  if (lt < S::R2)
+  {
+    float2 a0[S::R1], a1[S::R1];
+#pragma unroll
+    for (int j = 0; j < S::R1; ++j)
+    {
+      const int r = (lt + S::R2 * j + in_add) & (L - 1);
+      const float4 v =
+          r < in_count ? B4[r * TP + cp] : make_float4(0.f, 0.f, 0.f, 0.f);
+      a0[j] = make_float2(v.x, v.y);
+      a1[j] = make_float2(v.z, v.w);
+    }
+    reg_fft<S::R1, Rm<L>::V, INV>(a0, w);
+    reg_fft<S::R1, Rm<L>::V, INV>(a1, w);
+    const int rho = (lt + in_add) & (S::R2 - 1);
+#pragma unroll
+    for (int k1 = 0; k1 < S::R1; ++k1)
+    {
+      float2 v0 = a0[k1], v1 = a1[k1];
+      if (k1 != 0)
+      {
+        float2 r = tw[(lt * k1) & (L - 1)];
+        if (INV)
+          r.y = -r.y;
+        v0 = cmul(v0, r);
+        v1 = cmul(v1, r);
+      }
+      B4[(k1 * S::R2 + rho) * TP + cp] = make_float4(v0.x, v0.y, v1.x, v1.y);
+    }
+  }
+  __syncthreads();
+  if (lt < S::R1)
+  {
+#pragma unroll
+    for (int u = 0; u < S::R2; ++u)
+    {
+      const float4 v =
+          B4[(lt * S::R2 + ((u + in_add) & (S::R2 - 1))) * TP + cp];
+      b0[u] = make_float2(v.x, v.y);
+      b1[u] = make_float2(v.z, v.w);
+    }
+    reg_fft<S::R2, Rm<L>::V, INV>(b0, w);
+    reg_fft<S::R2, Rm<L>::V, INV>(b1, w);
+  }
+}
+
 // Tile t of a pass over `planes` planes of n_ct column tiles (PAIRED 0:
 // plane t / n_ct, columns (t % n_ct) * TC ...).  PAIRED > 0: a tile holds
 // TC / 2 columns of both planes (coils) of a pair; output element (plane c,
@@ -199,8 +259,8 @@ __device__ __forceinline__ void col_tile_fft(float2 *B, int cl, int lt,
 // layout of PAIRED 0, read without bank conflicts.  `tail` (PAIRED 2)
 // covers an odd last coil (pair tail_pl) with a one-coil map whose second
 // coil is out of range (zero fill).
-template <int L, bool INV, int PAIRED>
-__global__ void __launch_bounds__(Shape<L>::CT, 3)
+template <int L, bool INV, int PAIRED, int CPT = 1>
+__global__ void __launch_bounds__(Shape<L>::CT / CPT, 3)
     k_fft_cols_tma(const __grid_constant__ CUtensorMap tmap,
                    const __grid_constant__ CUtensorMap tail, long long tail_pl,
                    float2 *__restrict__ dst, long long ncols, FastDiv n_ct,
@@ -268,7 +328,10 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
   __syncthreads();
   float2 w[Rm<L>::V / 2];
   load_reg_roots<L>(w, tw);
-  const int cl = threadIdx.x % TC, lt = threadIdx.x / TC;
+  static_assert(CPT == 1 || (CPT == 2 && PAIRED == 2), "column pairs");
+  // CPT 2 (interleaved coil pairs): thread (cl = column pair, lt) runs tile
+  // columns 2 cl, 2 cl + 1, two adjacent grid columns of one coil
+  const int cl = threadIdx.x % (TC / CPT), lt = threadIdx.x / (TC / CPT);
   int i = 0;
   for (int t = blockIdx.x; t < n_tiles; t += stride, ++i)
   {
@@ -293,27 +356,55 @@ __global__ void __launch_bounds__(Shape<L>::CT, 3)
     }
     int pl, ct;
     tile(t, pl, ct);
-    const long long plane = PAIRED ? 2LL * pl + cl / CW : pl;
-    const long long col = (long long)ct * CW + cl % CW;
-    uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
-    if (colrange && col < ncols)
-      cr = __ldg(colrange + col);
-    const bool on = col < ncols && cr.x <= cr.y;
-    float2 bv[S::R2];
-    col_tile_fft<L, INV, PAIRED == 1>(buf + (size_t)b * L * TC, cl, lt,
-                                      in_add, in_count, w, tw, bv);
-    if (lt < S::R1 && on)
+    const int q = cl * CPT;  // first tile column of the thread
+    const long long plane = PAIRED ? 2LL * pl + q / CW : pl;
+    const long long col = (long long)ct * CW + q % CW;
+    const long long psz = (long long)dst_rows * ncols;
+    float2 *dp = PAIRED ? dst + ((plane >> 1) * psz + col) * 2 + (plane & 1)
+                        : dst + plane * psz + col;
+    const long long rs = PAIRED ? 2 * ncols : ncols;
+    if constexpr (CPT == 1)
     {
-      const long long psz = (long long)dst_rows * ncols;
-      float2 *dp = PAIRED ? dst + ((plane >> 1) * psz + col) * 2 + (plane & 1)
-                          : dst + plane * psz + col;
-      const long long rs = PAIRED ? 2 * ncols : ncols;
-#pragma unroll
-      for (int k2 = 0; k2 < S::R2; ++k2)
+      uint2 cr = make_uint2(0u, 0xFFFFFFFFu);
+      if (colrange && col < ncols)
+        cr = __ldg(colrange + col);
+      const bool on = col < ncols && cr.x <= cr.y;
+      float2 bv[S::R2];
+      col_tile_fft<L, INV, PAIRED == 1>(buf + (size_t)b * L * TC, cl, lt,
+                                        in_add, in_count, w, tw, bv);
+      if (lt < S::R1 && on)
       {
-        const int r = (lt + S::R1 * k2 + out_add) & (L - 1);
-        if (r < out_count && (unsigned)r >= cr.x && (unsigned)r <= cr.y)
-          dp[(long long)r * rs] = bv[k2];
+#pragma unroll
+        for (int k2 = 0; k2 < S::R2; ++k2)
+        {
+          const int r = (lt + S::R1 * k2 + out_add) & (L - 1);
+          if (r < out_count && (unsigned)r >= cr.x && (unsigned)r <= cr.y)
+            dp[(long long)r * rs] = bv[k2];
+        }
+      }
+    }
+    else
+    {  // columns col, col + 1 (ncols is even, so both or neither exist)
+      uint2 cr0 = make_uint2(0u, 0xFFFFFFFFu), cr1 = cr0;
+      if (colrange && col < ncols)
+      {
+        cr0 = __ldg(colrange + col);
+        cr1 = __ldg(colrange + col + 1);
+      }
+      float2 b0[S::R2], b1[S::R2];
+      col_tile_fft2<L, INV>(buf + (size_t)b * L * TC, cl, lt, in_add,
+                            in_count, w, tw, b0, b1);
+      if (lt < S::R1 && col < ncols)
+      {
+#pragma unroll
+        for (int k2 = 0; k2 < S::R2; ++k2)
+        {
+          const int r = (lt + S::R1 * k2 + out_add) & (L - 1);
+          if (r < out_count && (unsigned)r >= cr0.x && (unsigned)r <= cr0.y)
+            dp[(long long)r * rs] = b0[k2];
+          if (r < out_count && (unsigned)r >= cr1.x && (unsigned)r <= cr1.y)
+            dp[(long long)r * rs + 2] = b1[k2];  // next column, same coil
+        }
       }
     }
     tma::fence_proxy_async();  // the in-place writes before the refill
@@ -1212,20 +1303,24 @@ void cols(int L, const float2 *src, float2 *dst, long long ncols,
         const long long n_tiles = n_ct * (paired ? (planes + 1) / 2 : planes);
         if (n_tiles >= (1LL << 31) - 2LL * persistent_blocks(n_tiles))
           return;  // tile indices are 31-bit
-        auto launch = [&](auto k) {
+        auto launch = [&](auto k, int threads) {
           set_smem(k, ColTma<LL>::smem());
-          k<<<persistent_blocks(n_tiles), S::CT, ColTma<LL>::smem(), s>>>(
+          k<<<persistent_blocks(n_tiles), threads, ColTma<LL>::smem(), s>>>(
               tm, tail, tail_pl, dst, ncols, FastDiv((uint32_t)n_ct),
               (int)n_tiles, box_rows, ncopy,
               dst_rows, in_add, in_count, out_add, out_count, roots, colrange,
               listed ? tiles : nullptr, wait);
         };
+        // the interleaved coil-pair pass (twice the lines of the others,
+        // bound by instruction issue) runs two adjacent columns per thread;
+        // the plain passes, closer to the DRAM bound, keep the warps of one
+        // column per thread
         if (mode == 2)
-          launch(k_fft_cols_tma<LL, INV, 2>);
+          launch(k_fft_cols_tma<LL, INV, 2, 2>, S::CT / 2);
         else if (mode == 1)
-          launch(k_fft_cols_tma<LL, INV, 1>);
+          launch(k_fft_cols_tma<LL, INV, 1>, S::CT);
         else
-          launch(k_fft_cols_tma<LL, INV, 0>);
+          launch(k_fft_cols_tma<LL, INV, 0>, S::CT);
         GN_LAUNCH_CHECK("pruned column transform (tensor-copy tiles)");
         done = true;
       }
