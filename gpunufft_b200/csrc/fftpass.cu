@@ -258,7 +258,8 @@ __device__ __forceinline__ void col_tile_fft2(float2 *B, int cp, int lt,
 // r holds TC / 2 columns of the first coil, then of the second -- the
 // layout of PAIRED 0, read without bank conflicts.  `tail` (PAIRED 2)
 // covers an odd last coil (pair tail_pl) with a one-coil map whose second
-// coil is out of range (zero fill).
+// coil is out of range (zero fill).  CPT 2 (PAIRED 2 only): each thread
+// runs two adjacent columns of one coil (col_tile_fft2), half the threads.
 template <int L, bool INV, int PAIRED, int CPT = 1>
 __global__ void __launch_bounds__(Shape<L>::CT / CPT, 3)
     k_fft_cols_tma(const __grid_constant__ CUtensorMap tmap,
