@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include "cplx.cuh"
 #include "f32x2.cuh"
 
 namespace gnufft
@@ -77,10 +78,6 @@ __host__ __device__ constexpr int bitrev(int i, int R)
   return r;
 }
 
-__device__ __forceinline__ float2 cmul(float2 a, float2 b)
-{
-  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
 
 __host__ __device__ constexpr int ilog2(int v)
 {

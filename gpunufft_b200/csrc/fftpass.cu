@@ -489,8 +489,9 @@ __global__ void __launch_bounds__(Shape<L>::CT, L <= 256 ? 3 : 1)
         if (SENS && stage == 2)
         {  // conj(S) * v, running coil sum (std_gpuNUFFT_kernels.cu:158-218)
           const float2 sv = __ldg(sens + c * N + px);
-          acc[k2].x += v.x * sv.x + v.y * sv.y;
-          acc[k2].y += v.y * sv.x - v.x * sv.y;
+          const float2 t = cmul_conj(v, sv);
+          acc[k2].x = __fadd_rn(acc[k2].x, t.x);
+          acc[k2].y = __fadd_rn(acc[k2].y, t.y);
         }
         else
           out[c * N + px] = v;
@@ -678,8 +679,9 @@ __global__ void __launch_bounds__(Shape<L>::CT, 2)
         v.x = __fmul_rn(v.x, d[k2]);
         v.y = __fmul_rn(v.y, d[k2]);
         const float2 sv = st[n * TC + cl];
-        acc[k2].x += v.x * sv.x + v.y * sv.y;
-        acc[k2].y += v.y * sv.x - v.x * sv.y;
+        const float2 t = cmul_conj(v, sv);
+        acc[k2].x = __fadd_rn(acc[k2].x, t.x);
+        acc[k2].y = __fadd_rn(acc[k2].y, t.y);
       }
     }
     tma::fence_proxy_async();  // the in-place writes before the refill
@@ -781,8 +783,7 @@ __global__ void __launch_bounds__(kFftThreads, L <= 256 ? 4 : 1)
         {  // sensMulKernel, then deapodization (std_gpuNUFFT_kernels.cu)
           const float2 x = __ldg(image + px);
           const float2 s = __ldg(sens + c * N + px);
-          v.x = x.x * s.x - x.y * s.y;
-          v.y = x.x * s.y + x.y * s.x;
+          v = cmul(x, s);
         }
         else
           v = __ldg(image + c * N + px);
@@ -934,8 +935,7 @@ __global__ void __launch_bounds__(kFftThreads, 3)
           {  // sensMulKernel, then deapodization (std_gpuNUFFT_kernels.cu)
             const float2 x = img[xp];
             const float2 sv = crow[xp];
-            v.x = x.x * sv.x - x.y * sv.y;
-            v.y = x.x * sv.y + x.y * sv.x;
+            v = cmul(x, sv);
           }
           else
             v = crow[xp];
@@ -1095,8 +1095,7 @@ __global__ void __launch_bounds__(kFftThreads, L <= 256 ? 3 : 1)
           v.x = __fmul_rn(v.x, d);
           v.y = __fmul_rn(v.y, d);
           const float2 s = __ldg(sens + c * N + px);
-          t.x = v.x * s.x + v.y * s.y;
-          t.y = v.y * s.x - v.x * s.y;
+          t = cmul_conj(v, s);
         }
         term[xp] = t;
       }

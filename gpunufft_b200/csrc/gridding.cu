@@ -759,7 +759,7 @@ __global__ void __launch_bounds__(kThreads, xfft_min_blocks(CG, L))
           {
             float2 r = tw[(lt * k1) & (L - 1)];
             r.y = -r.y;
-            v = fftcore::cmul(v, r);
+            v = cmul(v, r);
           }
           acc[acc_pos<CG, SR2>(k1 * S::R2 + lt, cl)] = v;
         }
@@ -1515,8 +1515,9 @@ __device__ __forceinline__ void finish_pixel(long long p,
         // conj(S) * v, then the running coil sum
         // (std_gpuNUFFT_kernels.cu:158-218)
         const float2 s = sens[p + (long long)c * N];
-        accx += v.x * s.x + v.y * s.y;
-        accy += v.y * s.x - v.x * s.y;
+        const float2 t = cmul_conj(v, s);
+        accx = __fadd_rn(accx, t.x);
+        accy = __fadd_rn(accy, t.y);
       }
       else
       {
@@ -1562,8 +1563,7 @@ __device__ __forceinline__ float2 prepare_value(const float2 *__restrict__ image
   {  // sensMulKernel (std_gpuNUFFT_kernels.cu:142-156)
     const float2 a = __ldg(image + p);
     const float2 s = __ldg(sens + p + cN);
-    v.x = a.x * s.x - a.y * s.y;
-    v.y = a.x * s.y + a.y * s.x;
+    v = cmul(a, s);
   }
   else
   {
