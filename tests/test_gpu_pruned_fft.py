@@ -77,3 +77,31 @@ def test_persistent_row_pass_equals_the_kernel_it_replaces():
         yp = part.forward(x)
         part.close()
         assert np.array_equal(yp.view(np.uint64), y[c0:c0 + 8].view(np.uint64))
+
+
+@pytest.mark.parametrize("C,maps", [(8, False), (5, False), (6, True)])
+def test_paired_forward_equals_plain_layout(C, maps):
+    """The default 3-D forward writes the grid with coil pairs interleaved:
+    its z pass copies one 4-D box per tile, transforms only the listed
+    column tiles and runs two columns per thread, and the interpolation
+    reads coil-pair tiles in the plan's lane order.  A plan with 8-coil
+    forward tiles keeps the plain layout (one column per thread, every
+    column tile, single-coil tiles).  Per coil the arithmetic is the same,
+    so the outputs must be bitwise equal (odd C: the last pair's second
+    coil is an out-of-range box)."""
+    import gpunufft_b200 as G
+    rng = np.random.default_rng(13 + C)
+    dims = (32, 32, 32)
+    traj = np.asarray(kooshball_3d(300, 64), np.float32)  # empty columns
+    dens = rng.uniform(0.2, 1.0, traj.shape[1]).astype(np.float32)
+    sens = gaussian_maps(C, dims[::-1], rng) if maps else None
+    x = cplx(rng, *dims[::-1]) if maps else cplx(rng, C, *dims[::-1])
+    paired = G.Plan(traj, dims, 3, 8, 2.0, dens, sens, G.BALANCED)
+    plain = G.Plan(traj, dims, 3, 8, 2.0, dens, sens, G.BALANCED,
+                   tile_coils=8)
+    try:
+        a, b = paired.forward(x), plain.forward(x)
+    finally:
+        paired.close()
+        plain.close()
+    assert np.array_equal(a.view(np.uint64), b.view(np.uint64))
