@@ -149,9 +149,10 @@ __device__ __forceinline__ void gather_inv_unit(
     tile[jl][cl] = v;
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < kGatherSamples * nc; i += kThreads)
-  {
-    const int cl = i % nc, jl = i / nc;
+  // one sample's coil row per nc consecutive threads (a whole block of
+  // coils: nc is a constant, so the row and lane are a shift and a mask)
+  auto put = [&](int i, int n) {
+    const int cl = i % n, jl = i / n;
     if (j0 + jl < M)
     {
       float2 v = tile[jl][cl];
@@ -162,7 +163,16 @@ __device__ __forceinline__ void gather_inv_unit(
       }
       ks[(size_t)s_t[jl] * CP + c0 + cl] = v;
     }
+  };
+  if (nc == kGatherCoils)
+  {
+#pragma unroll
+    for (int i = threadIdx.x; i < kGatherSamples * kGatherCoils; i += kThreads)
+      put(i, kGatherCoils);
   }
+  else
+    for (int i = threadIdx.x; i < kGatherSamples * nc; i += kThreads)
+      put(i, nc);
 }
 
 __global__ void __launch_bounds__(kThreads)
