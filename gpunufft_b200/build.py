@@ -72,7 +72,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     objs = [_obj(s) for s in srcs]
     if todo or not os.path.exists(LIB):
         cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + [
-            "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft", "-lcudart",
+            "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcufft", "-lcudart", "-lpthread",
             "-Xlinker", "-rpath", "-Xlinker",
             os.path.join(CUDA_HOME, "lib64")]
         r = subprocess.run(cmd, capture_output=True, text=True)

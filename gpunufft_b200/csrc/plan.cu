@@ -32,6 +32,7 @@
 #include "footprint.cuh"
 #include "geometry.hpp"
 #include "gridding.cuh"
+#include "hostcopy.hpp"
 #include "planview.hpp"
 #include "tma.cuh"
 #include "trajgrad.cuh"
@@ -371,9 +372,8 @@ void set_sens_host(gnufft_plan &p, const void *sens, uint32_t n_coils)
   // keep the device buffer when it is large enough (no free / malloc, which
   // would synchronise the device, when maps are swapped between requests)
   p.sens.ensure(n * sizeof(float2));
-  GN_CUDA(cudaMemcpyAsync(p.sens.get(), p.plain ? p.sens_h.data() : s,
-                          n * sizeof(float2), cudaMemcpyHostToDevice,
-                          p.stream));
+  copy_host_to_device(p.sens.get(), p.plain ? p.sens_h.data() : s,
+                      n * sizeof(float2), p.stream);
   p.sens_coils = n_coils;
 }
 
@@ -1340,12 +1340,10 @@ gnufft_status gnufft_adjoint_host(gnufft_plan *p, const void *kspace,
     const size_t nout = adjoint_out_count(*p, n_coils, output);
     p->stage_in.ensure(nin * sizeof(float2));
     p->stage_out.ensure(nout * sizeof(float2));
-    GN_CUDA(cudaMemcpyAsync(p->stage_in.get(), kspace, nin * sizeof(float2),
-                            cudaMemcpyHostToDevice, s));
+    copy_host_to_device(p->stage_in.get(), kspace, nin * sizeof(float2), s);
     adjoint_chunked(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
                     n_coils, output, s);
-    GN_CUDA(cudaMemcpyAsync(image, p->stage_out.get(), nout * sizeof(float2),
-                            cudaMemcpyDeviceToHost, s));
+    copy_device_to_host(image, p->stage_out.get(), nout * sizeof(float2), s);
     GN_CUDA(cudaStreamSynchronize(s));
     collect_times(*p, s);
     check_copy_err(*p);  // this call's own tile copies
@@ -1370,8 +1368,7 @@ gnufft_status gnufft_forward_host(gnufft_plan *p, const void *image,
     const size_t nout = (size_t)n_coils * p->M;
     p->stage_in.ensure(nin * sizeof(float2));
     p->stage_out.ensure(nout * sizeof(float2));
-    GN_CUDA(cudaMemcpyAsync(p->stage_in.get(), image, nin * sizeof(float2),
-                            cudaMemcpyHostToDevice, s));
+    copy_host_to_device(p->stage_in.get(), image, nin * sizeof(float2), s);
     if (p->plain)
     {
       gnufft_status st = gnufft_forward_device(p, p->stage_in.get(),
@@ -1383,8 +1380,7 @@ gnufft_status gnufft_forward_host(gnufft_plan *p, const void *image,
     else
       forward_chunked(*p, p->stage_in.as<float2>(), p->stage_out.as<float2>(),
                       n_coils, output, s);
-    GN_CUDA(cudaMemcpyAsync(kspace, p->stage_out.get(), nout * sizeof(float2),
-                            cudaMemcpyDeviceToHost, s));
+    copy_device_to_host(kspace, p->stage_out.get(), nout * sizeof(float2), s);
     GN_CUDA(cudaStreamSynchronize(s));
     collect_times(*p, s);
     check_copy_err(*p);  // this call's own tile copies
