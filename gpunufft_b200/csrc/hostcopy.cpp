@@ -20,12 +20,13 @@ constexpr int kMaxDevices = 64;
 
 struct Ring
 {
+  std::mutex m;  // one staged copy at a time per device
   bool tried = false, ok = false;
   char *buf[2] = {nullptr, nullptr};
   cudaEvent_t ev[2] = {nullptr, nullptr};
 };
 
-std::mutex g_mutex;  // one staged copy at a time (guards the rings)
+std::mutex g_init;  // guards the rings' allocation
 Ring g_rings[kMaxDevices];
 
 // The current device's ring, allocated on first use and kept for the
@@ -37,6 +38,7 @@ Ring *ring()
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return nullptr;
   Ring &r = g_rings[dev];
+  std::lock_guard<std::mutex> lock(g_init);
   if (!r.tried)
   {
     r.tried = true;
@@ -65,19 +67,31 @@ Ring *ring()
 }
 
 // memcpy of len bytes split over kCopyThreads threads (the caller's one
-// of them).
+// of them; parts whose thread cannot be started are copied by the caller).
 void parallel_copy(char *dst, const char *src, size_t len)
 {
   const size_t part = (len + kCopyThreads - 1) / kCopyThreads;
-  std::vector<std::thread> th;
-  for (int k = 1; k < kCopyThreads; ++k)
-  {
+  auto copy_part = [=](int k) {
     const size_t o = (size_t)k * part;
-    if (o >= len)
-      break;
-    th.emplace_back([=] { std::memcpy(dst + o, src + o, std::min(part, len - o)); });
+    if (o < len)
+      std::memcpy(dst + o, src + o, std::min(part, len - o));
+  };
+  std::vector<std::thread> th;
+  int k = 1;
+  for (; k < kCopyThreads && (size_t)k * part < len; ++k)
+  {
+    try
+    {
+      th.emplace_back(copy_part, k);
+    }
+    catch (...)
+    {
+      break;  // no more threads: the rest below, on this one
+    }
   }
-  std::memcpy(dst, src, std::min(part, len));
+  for (int q = k; q < kCopyThreads; ++q)
+    copy_part(q);
+  copy_part(0);
   for (auto &t : th)
     t.join();
 }
@@ -88,13 +102,13 @@ void copy_host_to_device(void *dst, const void *src, size_t bytes,
 {
   if (!bytes)
     return;
-  std::lock_guard<std::mutex> lock(g_mutex);
   Ring *r = bytes >= kSmall ? ring() : nullptr;
   if (!r)
   {
     GN_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
     return;
   }
+  std::lock_guard<std::mutex> lock(r->m);
   char *d = static_cast<char *>(dst);
   const char *h = static_cast<const char *>(src);
   for (size_t off = 0, i = 0; off < bytes; off += kChunk, ++i)
@@ -114,7 +128,6 @@ void copy_device_to_host(void *dst, const void *src, size_t bytes,
 {
   if (!bytes)
     return;
-  std::lock_guard<std::mutex> lock(g_mutex);
   Ring *r = bytes >= kSmall ? ring() : nullptr;
   if (!r)
   {
@@ -122,6 +135,7 @@ void copy_device_to_host(void *dst, const void *src, size_t bytes,
     GN_CUDA(cudaStreamSynchronize(s));
     return;
   }
+  std::lock_guard<std::mutex> lock(r->m);
   char *h = static_cast<char *>(dst);
   const char *d = static_cast<const char *>(src);
   size_t prev_off = 0, prev_len = 0;
