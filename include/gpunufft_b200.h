@@ -200,7 +200,12 @@ GNUFFT_API gnufft_status gnufft_set_sens_device(gnufft_plan *plan,
  *   DEAPODIZATION: [image] coil-combined when the plan has sensitivity
  *                  maps, else [n_coils][image].
  * _host: host buffers, synchronous.  _device: device buffers, ordered on
- * `stream` (a cudaStream_t; NULL = the legacy default stream). */
+ * `stream` (a cudaStream_t; NULL = the legacy default stream).
+ * Host arrays of 16 MB or more (and host sensitivity maps given to
+ * gnufft_set_sens / gnufft_plan_create) are copied through a process-wide
+ * ring of two 8 MB pinned buffers per device, allocated on first use and
+ * kept until the process ends, filled and drained by up to four short-lived
+ * host threads per chunk; smaller ones with one pageable copy. */
 GNUFFT_API gnufft_status gnufft_adjoint_host(gnufft_plan *plan, const void *kspace,
                                   void *image, uint32_t n_coils,
                                   int32_t output);
