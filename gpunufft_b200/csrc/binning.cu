@@ -270,8 +270,14 @@ int bits_for(uint32_t max_value)
 }
 }  // namespace
 
+size_t scan_scratch_elems(size_t n)
+{
+  const size_t nb = (n + kScanTile - 1) / kScanTile;
+  return nb <= 1 ? 0 : nb + scan_scratch_elems(nb);
+}
+
 void scan_exclusive(const uint32_t *in, uint32_t *out, size_t n,
-                    cudaStream_t s)
+                    cudaStream_t s, uint32_t *scratch)
 {
   if (n == 0)
     return;
@@ -282,15 +288,20 @@ void scan_exclusive(const uint32_t *in, uint32_t *out, size_t n,
     GN_LAUNCH_CHECK("scan");
     return;
   }
-  DeviceBuffer sums(nb * sizeof(uint32_t));
-  k_scan_tile<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out,
-                                                     sums.as<uint32_t>(), n);
+  DeviceBuffer own;
+  if (!scratch)
+  {
+    own.reset(scan_scratch_elems(n) * sizeof(uint32_t));
+    scratch = own.as<uint32_t>();
+  }
+  uint32_t *sums = scratch;  // this level's block sums, then the next level's
+  k_scan_tile<<<(unsigned)nb, kScanThreads, 0, s>>>(in, out, sums, n);
   GN_LAUNCH_CHECK("scan");
-  scan_exclusive(sums.as<uint32_t>(), sums.as<uint32_t>(), nb, s);
-  k_scan_add<<<(unsigned)nb, kScanThreads, 0, s>>>(out, sums.as<uint32_t>(),
-                                                   n);
+  scan_exclusive(sums, sums, nb, s, sums + nb);
+  k_scan_add<<<(unsigned)nb, kScanThreads, 0, s>>>(out, sums, n);
   GN_LAUNCH_CHECK("scan add");
-  GN_CUDA(cudaStreamSynchronize(s));  // `sums` is released on return
+  if (own.get())
+    GN_CUDA(cudaStreamSynchronize(s));  // `own` is released on return
 }
 
 void sort_pairs(const uint32_t *keys_in, const uint32_t *vals_in,
@@ -303,27 +314,30 @@ void sort_pairs(const uint32_t *keys_in, const uint32_t *vals_in,
     throw Error(kNotSupported, "more than 2^32 items to sort");
   const int passes = (key_bits + 7) / 8;
   const unsigned nb = (unsigned)((n + kSortTile - 1) / kSortTile);
-  DeviceBuffer hist((size_t)256 * nb * sizeof(uint32_t));
-  DeviceBuffer tk(n * sizeof(uint32_t)), tv(n * sizeof(uint32_t));
+  // one allocation: histograms, their scan scratch, ping-pong keys / values
+  const size_t nh = (size_t)256 * nb, nsc = scan_scratch_elems(nh);
+  const size_t off_tk = (nh + nsc + 63) / 64 * 64;  // 256-byte aligned
+  const size_t off_tv = off_tk + (n + 63) / 64 * 64;
+  DeviceBuffer work((off_tv + n) * sizeof(uint32_t));
+  uint32_t *hist = work.as<uint32_t>(), *scratch = hist + nh;
+  uint32_t *tk = hist + off_tk, *tv = hist + off_tv;
   // ping-pong so that the last pass lands in *_out
   const uint32_t *ki = keys_in, *vi = vals_in;
   for (int p = 0; p < passes; ++p)
   {
     const bool to_out = ((passes - 1 - p) % 2) == 0;
-    uint32_t *ko = to_out ? keys_out : tk.as<uint32_t>();
-    uint32_t *vo = to_out ? vals_out : tv.as<uint32_t>();
-    k_radix_hist<<<nb, kSortThreads, 0, s>>>(ki, n, 8 * p,
-                                             hist.as<uint32_t>());
+    uint32_t *ko = to_out ? keys_out : tk;
+    uint32_t *vo = to_out ? vals_out : tv;
+    k_radix_hist<<<nb, kSortThreads, 0, s>>>(ki, n, 8 * p, hist);
     GN_LAUNCH_CHECK("radix hist");
-    scan_exclusive(hist.as<uint32_t>(), hist.as<uint32_t>(), (size_t)256 * nb,
-                   s);
+    scan_exclusive(hist, hist, nh, s, scratch);
     k_radix_scatter<<<nb, kSortThreads, 0, s>>>(ki, vi, ko, vo, n, 8 * p,
-                                                hist.as<uint32_t>());
+                                                hist);
     GN_LAUNCH_CHECK("radix scatter");
     ki = ko;
     vi = vo;
   }
-  GN_CUDA(cudaStreamSynchronize(s));
+  GN_CUDA(cudaStreamSynchronize(s));  // `work` is released on return
 }
 
 void histogram_offsets(const uint32_t *keys, size_t n, uint32_t bins,
@@ -373,7 +387,8 @@ size_t build_interp_matrix(const float *traj_sorted,
     nz.reset(sizeof(uint2));
     return 0;
   }
-  DeviceBuffer count((size_t)(M + 1) * sizeof(uint32_t));
+  const size_t nsc = scan_scratch_elems((size_t)M + 1);
+  DeviceBuffer count(((size_t)M + 1 + nsc) * sizeof(uint32_t));
   GN_CUDA(cudaMemsetAsync(count.get(), 0, (size_t)(M + 1) * 4, s));
   const unsigned nb = grid_for(M, 256, 8192);
   k_interp_pairs<false><<<nb, 256, 0, s>>>(traj_sorted, sector_sorted, M, g,
@@ -381,7 +396,7 @@ size_t build_interp_matrix(const float *traj_sorted,
                                            nullptr, nullptr, nullptr);
   GN_LAUNCH_CHECK("interp count");
   scan_exclusive(count.as<uint32_t>(), count.as<uint32_t>(), (size_t)M + 1,
-                 s);
+                 s, count.as<uint32_t>() + M + 1);
   uint32_t total = 0;
   GN_CUDA(cudaMemcpyAsync(&total, count.as<uint32_t>() + M, sizeof(uint32_t),
                           cudaMemcpyDeviceToHost, s));

@@ -12,9 +12,12 @@
 namespace gnufft
 {
 
-// Exclusive prefix sum of n u32 values (in may equal out).
+// Exclusive prefix sum of n u32 values (in may equal out).  `scratch`
+// (device, scan_scratch_elems(n) u32, or NULL) holds the block sums; with
+// NULL the call allocates them and synchronises the stream before freeing.
 void scan_exclusive(const uint32_t *in, uint32_t *out, size_t n,
-                    cudaStream_t s);
+                    cudaStream_t s, uint32_t *scratch = nullptr);
+size_t scan_scratch_elems(size_t n);
 
 // Stable LSD radix sort of (key, value) pairs on the low `key_bits` bits of
 // the keys.  Sorted output ends in keys_out / vals_out.
