@@ -469,7 +469,7 @@ def run_gpu_arm(args, rank, world, dist):
     for kname, (what, kms, nbytes) in kernels.items():
         ach = nbytes / (kms * 1e-3) / 1e9
         traffic, tsrc = profile_traffic(args.workload, kname)
-        # the gridding bytes as the survey counts them for either direction:
+        # the gridding bytes of either direction counted as 8MC + 4dM + 8GC:
         # k-space, coordinates and the oversampled grid once each
         sach = gbytes / (kms * 1e-3) / 1e9
         rooflines.append({
